@@ -1,0 +1,160 @@
+/*
+ * mcb200.h — C ABI of the B200 (sm_100a) implementation of MCmatlab's two hot paths.
+ *
+ * Plain C types only: host pointers, sizes and POD structs. Every entry point returns
+ * an mcb_status; on failure mcb_last_error(ctx) holds a message. No entry point
+ * prints, aborts or longjmps.
+ *
+ * Array layout follows MATLAB: column-major, x fastest. A grid array has
+ * nx*ny*nz elements; a per-wavelength grid has nx*ny*nz*nL.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   mcb_mc_run        <- mexFunction of +MCmatlab/src/MCmatlab.c:317-791
+ *                        (called as MCmatlab(model,1) / MCmatlab_CUDA(model,1),
+ *                         +MCmatlab/@model/runMonteCarlo.m:99-104, :169-174)
+ *   mcb_heat_forward  <- mexFunction of +MCmatlab/src/finiteElementHeatPropagator.c:688-821
+ *                        (called from +MCmatlab/@model/simulateHeatDistribution.m:259-264,
+ *                         :320-325, :381-386)
+ * The remaining entry points (batched MC, perturbation-MC gradients, the heat
+ * adjoint, device-resident heat state) have no counterpart in the reference; each
+ * says so below.
+ */
+#ifndef MCB200_H
+#define MCB200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  MCB_OK = 0,
+  MCB_EINVAL = 1,     /* invalid argument or model */
+  MCB_ENOMEM = 2,     /* device or host allocation failed */
+  MCB_ECUDA = 3,      /* CUDA runtime error */
+  MCB_ECANCELLED = 4, /* cancel flag was set during the run */
+  MCB_ETIMEOUT = 5,   /* a bounded device-side wait gave up */
+  MCB_ELAUNCH = 6     /* all packets launched outside the allowed region (MCmatlab.c:745) */
+} mcb_status;
+
+typedef struct mcb_ctx mcb_ctx;
+
+/* One context per device and caller thread; it owns device buffers reused across calls. */
+mcb_status mcb_ctx_create(int device, mcb_ctx **out);
+mcb_status mcb_ctx_destroy(mcb_ctx *ctx);
+const char *mcb_last_error(const mcb_ctx *ctx);
+/* Host-visible cancel flag polled by the transport kernel (stands in for utIsInterruptPending,
+ * MCmatlab.c:293-298). Setting *flag != 0 makes the running mcb_mc_run return MCB_ECANCELLED. */
+volatile int *mcb_cancel_flag(mcb_ctx *ctx);
+
+/* ------------------------------------------------------------------------------------------
+ * Monte Carlo photon transport.
+ * mcb_mc_model carries exactly the model properties MCmatlab.c's mexFunction reads, in their
+ * MATLAB meaning (MCmatlab.c:317-616), plus a seed for the counter-based RNG.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct mcb_distr {
+  const double *values; /* custom distribution samples, or NULL */
+  int64_t n;            /* number of samples; n == 1 means values[0] is a code: 0 top-hat, 1 Gaussian, 2 Lambertian */
+  double width;         /* radialWidth / XWidth / YWidth */
+} mcb_distr;
+
+typedef struct mcb_mc_model {
+  /* geometry (model.G and model.MC.M) */
+  int32_t nx, ny, nz;
+  double dx, dy, dz;
+  const uint8_t *M;              /* [nx*ny*nz], 1-based sub-medium index (model.MC.M) */
+  /* media (model.MC.mediaProperties), column-major [nM x nL] */
+  int32_t nM, nL;
+  const double *mua, *mus, *g, *n, *CDFidx; /* g NaN -> custom phase function CDFs[:, CDFidx] */
+  const double *CDFs;            /* [201 x nCDF] or NULL */
+  int64_t nCDFelems;             /* 201 * nCDF */
+  const float *interfaceNormals; /* [2 x nx*ny*nz] (theta, phi) or NULL when matchedInterfaces */
+  const float *sourceDistribution; /* [nx*ny*nz*nL] distributed source, or NULL */
+  const double *spectrum;        /* [nL] power fraction per wavelength (model.MC.spectrum) */
+  /* run control */
+  double nPhotonsRequested;      /* NaN: timed run of simulationTimeRequested minutes */
+  double simulationTimeRequested;
+  int32_t requestCollectedPhotons;
+  int32_t calcNFR;
+  int32_t useLightCollector;
+  int32_t farFieldRes;
+  int32_t boundaryType;          /* 0 none escaping, 1 all faces, 2 top only, 3 top/bottom + cyclic x/y */
+  int32_t nExamplePaths;
+  uint64_t seed;                 /* Philox-4x32-10 key */
+  /* light source (model.MC.LS) */
+  int32_t sourceType;            /* 0..5, ignored when sourceDistribution != NULL */
+  double xFocus, yFocus, zFocus, theta, phi, psi, emitterLength;
+  mcb_distr FPID_radial, FPID_X, FPID_Y, AID_radial, AID_X, AID_Y;
+  /* light collector (model.MC.LC) */
+  double LC_x, LC_y, LC_z, LC_theta, LC_phi, LC_f, LC_diam, LC_fieldSize, LC_NA;
+  double LC_tStart, LC_tEnd;
+  int32_t LC_res, LC_nTimeBins;
+  /* deposition criteria (model.MC.depositionCriteria); +inf allowed for the maxima */
+  double DC_minScatterings, DC_maxScatterings, DC_minRefractions, DC_maxRefractions;
+  double DC_minReflections, DC_maxReflections, DC_minInterfaceTransitions, DC_maxInterfaceTransitions;
+  double DC_minSubmediaIdx, DC_maxSubmediaIdx; /* 1-based */
+  int32_t DC_onlyCollected, DC_evaluateOnlyAtEndOfLife;
+} mcb_mc_model;
+
+typedef struct mcb_mc_result {
+  /* caller-owned output arrays (NULL = not wanted); sizes as the MEX allocates them (MCmatlab.c:461-493) */
+  float *NFR;        /* [nx*ny*nz*nL] normalised fluence rate (when calcNFR) */
+  float *image;      /* [res*res*(nTimeBins ? nTimeBins+2 : 1)*nL] (when useLightCollector) */
+  float *farField;   /* [farFieldRes^2*nL] */
+  float *NI_xpos, *NI_xneg, *NI_ypos, *NI_yneg; /* [ny*nz*nL], [nx*nz*nL] (boundaryType 1) */
+  float *NI_zpos;    /* [nx*ny*nL] (boundaryType 1, 3) */
+  float *NI_zneg;    /* [nx*ny*nL] (1, 3) or [5nx*5ny*nL] (2) */
+  double *examplePaths;     /* [4 x examplePathsCap] x,y,z,weight columns, NaN-separated */
+  int64_t examplePathsCap;  /* capacity in columns */
+  /* results */
+  int64_t examplePathsN;    /* columns written */
+  double nPhotons, nPhotonsCollected, nThreads, simulationTime; /* simulationTime in minutes */
+  /* kernel statistics (not in the reference) */
+  uint64_t propagationSteps;   /* propagatePhoton-equivalent sub-steps executed */
+  double kernelMs;             /* device time of the transport kernels */
+} mcb_mc_result;
+
+/* Replaces MCmatlab.c mexFunction: runs all wavelengths, normalises and writes the outputs. */
+mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_result *result);
+
+/* No counterpart in the reference: runs n independent models (different grids, media,
+ * wavelengths, photon counts) in one persistent launch. Results equal n calls of mcb_mc_run
+ * up to FP64 summation order. */
+mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,
+                            mcb_mc_result *const *results);
+
+/* ------------------------------------------------------------------------------------------
+ * Heat diffusion (Douglas-Gunn ADI) with Arrhenius damage.
+ * mcb_heat_params carries the fields of heatSimParameters read by
+ * finiteElementHeatPropagator.c:688-739.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct mcb_heat_params {
+  int32_t nx, ny, nz, nM;
+  const uint8_t *M;             /* [nx*ny*nz] 0-based medium index (model.HS.M - 1) */
+  const float *dTdtperdeltaT;   /* [nM x nM x 3] column-major: c(i,j,d) = TC_eff(i,j)/VHC_i/d_d^2 */
+  const float *dTdt_abs;        /* [nx*ny*nz] heating rate while the light is on [K/s] */
+  const double *A, *E;          /* [nM] Arrhenius frequency factor [1/s] and activation energy [J/mol] */
+  int32_t lightsOn;
+  int32_t heatBoundaryType;     /* 0 insulating, 1 constant-temperature (heat-sinked) faces */
+  int64_t steps;                /* nt */
+  double dt;
+  int32_t nSensors;
+  const double *tempSensorCornerIdxs;    /* [nSensors] 0-based linear corner index */
+  const double *tempSensorInterpWeights; /* [nSensors x 3] column-major (wx, wy, wz) */
+} mcb_heat_params;
+
+/* Replaces finiteElementHeatPropagator.c mexFunction.
+ *   T            in/out [nx*ny*nz]
+ *   Omega        in/out [nx*ny*nz], or NULL for no damage (the MEX's NaN-scalar Omega)
+ *   sensorTemps  out [nSensors x (steps+1)] (may be NULL when nSensors == 0)
+ *   maxMediaTemps out [nM]: max over all voxels of medium m and all steps of T (-inf if none) */
+mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
+                            double *sensorTemps, float *maxMediaTemps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCB200_H */

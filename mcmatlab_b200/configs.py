@@ -1,0 +1,147 @@
+"""Synthetic, seeded workload definitions used by the tests and the benchmark.
+
+No public dataset is involved; each workload is generated from its description:
+
+* standard_tissue_cube(n)  — cube of side 0.1 cm with n^3 voxels: air above z = 0.01 cm,
+  an epidermis-like layer to z = 0.016 cm, dermis below, and a y-aligned vessel of
+  radius 0.01 cm centred at x = 0 (centred coordinates), z = 0.04 cm. Pencil beam at
+  the centre, all cuboid faces escaping, refractive index mismatches on.
+* heat_on_cube(...)        — thermal properties for the same geometry (tissue VHC 3.9,
+  TC 0.0037; air VHC 0.0012, TC 0.00026), damage (E = 4.48e5, A = 7.6e66) in the vessel.
+* batched_sweep(...)       — seeded instances of layered media + one cylinder with
+  randomised grids, wavelengths and optical properties.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import model as mm
+
+
+def _tissue_media(params):
+    air = mm.mediumProperties(name="air", mua=1e-8, mus=1e-8, g=1.0, n=1.0, VHC=0.0012, TC=0.00026)
+    epi = mm.mediumProperties(name="epidermis", mua=10.0, mus=150.0, g=0.9, n=1.3, VHC=3.9, TC=0.0037)
+    der = mm.mediumProperties(name="dermis", mua=1.0, mus=100.0, g=0.9, n=1.3, VHC=3.9, TC=0.0037)
+    ves = mm.mediumProperties(name="blood vessel", mua=200.0, mus=100.0, g=0.9, n=1.3, VHC=3.9, TC=0.0037,
+                              E=4.48e5, A=7.6e66)
+    return [air, epi, der, ves]
+
+
+def _tissue_geom(X, Y, Z, params):
+    M = np.full(X.shape, 3.0)
+    M[Z < 0.016] = 2
+    M[Z < 0.01] = 1
+    M[(X - 0.0) ** 2 + (Z - 0.04) ** 2 < 0.01 ** 2] = 4
+    return M
+
+
+def standard_tissue_cube(n=100, nPhotons=1e6, seed=1, matched=False):
+    m = mm.model()
+    m.G.nx = m.G.ny = m.G.nz = n
+    m.G.Lx = m.G.Ly = m.G.Lz = 0.1
+    m.G.mediaPropertiesFunc = _tissue_media
+    m.G.geomFunc = _tissue_geom
+    m.MC.nPhotonsRequested = nPhotons
+    m.MC.seed = seed
+    m.MC.matchedInterfaces = matched
+    m.MC.boundaryType = 1
+    m.MC.wavelength = 532.0
+    m.MC.lightSource.sourceType = 0
+    m.MC.silentMode = True
+    m.G.updateGeometry()
+    return m
+
+
+def heat_on_cube(m, durationOn=0.5, durationOff=0.5, nUpdates=10, dtFactor=0.9):
+    m.HS.T = 37.0
+    m.HS.durationOn = durationOn
+    m.HS.durationOff = durationOff
+    m.HS.nUpdates = nUpdates
+    m.HS.heatBoundaryType = 0
+    m.HS.dtFactor = dtFactor
+    m.HS.silentMode = True
+    return m
+
+
+def _layered_media_factory(rng, wavelengths):
+    """Three layers plus one cylinder; per-medium mua log-uniform(0.1, 300)/cm per wavelength,
+    mus = a (lambda/500 nm)^-b, g in [0.7, 0.95], n in {1.0, 1.37, 1.4}."""
+    nmed = 4
+    mua_tab = {float(w): np.exp(rng.uniform(np.log(0.1), np.log(300.0), nmed)) for w in wavelengths}
+    a = rng.uniform(50.0, 300.0, nmed)
+    b = rng.uniform(0.5, 2.0, nmed)
+    g = rng.uniform(0.7, 0.95, nmed)
+    nvals = np.array([1.0, 1.37, 1.4])
+    n = nvals[rng.integers(0, 3, nmed)]
+    n[0] = 1.0  # top layer index-matched to the outside so packets can escape through it
+
+    def media(params):
+        out = []
+        for k in range(nmed):
+            out.append(mm.mediumProperties(
+                name="medium%d" % k,
+                mua=(lambda wl, k=k: mua_tab[float(wl)][k]),
+                mus=(lambda wl, k=k: a[k] * (wl / 500.0) ** (-b[k])),
+                g=float(g[k]), n=float(n[k])))
+        return out
+    return media
+
+
+def batched_sweep(n_instances=64, seed=7, min_grid=(64, 64, 64), max_grid=(200, 200, 150),
+                  photons=(1e5, 1e7), scale=1.0):
+    """Seeded instances for a batched launch (grids, wavelengths, media, photon counts, Gaussian beams).
+
+    Half the instances add time tagging (64 bins to 1 ns on a fibre light collector) and cyclic
+    x/y boundaries. `scale` multiplies photon counts (tests use small values).
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_instances):
+        nx = int(rng.integers(min_grid[0], max_grid[0] + 1))
+        ny = int(rng.integers(min_grid[1], max_grid[1] + 1))
+        nz = int(rng.integers(min_grid[2], max_grid[2] + 1))
+        wl = float(rng.uniform(450.0, 900.0))
+        m = mm.model()
+        m.G.nx, m.G.ny, m.G.nz = nx, ny, nz
+        m.G.Lx = m.G.Ly = 0.2
+        m.G.Lz = 0.15
+        m.G.mediaPropertiesFunc = _layered_media_factory(rng, [wl])
+        t1, t2 = sorted(rng.uniform(0.01, 0.08, 2))
+        cz = float(rng.uniform(0.05, 0.12))
+        r = float(rng.uniform(0.005, 0.02))
+
+        def geom(X, Y, Z, p, t1=t1, t2=t2, cz=cz, r=r):
+            M = np.full(X.shape, 3.0)
+            M[Z < t2] = 2
+            M[Z < t1] = 1
+            M[X ** 2 + (Z - cz) ** 2 < r ** 2] = 4
+            return M
+        m.G.geomFunc = geom
+        m.MC.wavelength = wl
+        m.MC.matchedInterfaces = False
+        m.MC.nPhotonsRequested = float(max(1000, round(math.exp(rng.uniform(math.log(photons[0]), math.log(photons[1]))) * scale)))
+        m.MC.seed = 1000 + i
+        m.MC.silentMode = True
+        m.MC.lightSource.sourceType = 4
+        m.MC.lightSource.FPID.radialDistr = 1
+        m.MC.lightSource.FPID.radialWidth = float(rng.uniform(0.005, 0.02))
+        m.MC.lightSource.AID.radialDistr = 1
+        m.MC.lightSource.AID.radialWidth = 0.0
+        if i % 2 == 1:
+            m.MC.boundaryType = 3
+            m.MC.useLightCollector = True
+            lc = m.MC.lightCollector
+            lc.x, lc.y, lc.z = 0.0, 0.0, -0.05
+            lc.theta, lc.phi = 0.0, math.pi / 2
+            lc.f = math.inf
+            lc.diam = 0.1
+            lc.NA = 0.5
+            lc.res = 1
+            lc.tStart, lc.tEnd, lc.nTimeBins = 0.0, 1e-9, 64
+        else:
+            m.MC.boundaryType = 1
+        m.G.updateGeometry()
+        out.append(m)
+    return out

@@ -1,0 +1,159 @@
+"""The MEX-level view of a model: what the reference's MEX functions read.
+
+`prepare_mc(model, simType)` performs the MATLAB-side steps of runMonteCarlo
+(+MCmatlab/@model/runMonteCarlo.m:51-66, :145-176) that happen before the MEX call and
+returns a flat dict `mc_in` of numpy arrays and scalars. `mex_model_tree(mc_in)`
+turns that dict into the nested property tree the MEX function reads with
+mxGetPropertyShared (+MCmatlab/src/MCmatlab.c:317-616), with MATLAB's types:
+Python bool -> logical, number -> double, numpy arrays keep their dtype.
+The same tree drives the reference MEX (through the oracle's mx shim) and this
+library's MEX shim, so both see identical inputs.
+
+`heat_mex_params(...)` builds the heatSimParameters struct of
++MCmatlab/@model/simulateHeatDistribution.m:209-211 as read by
++MCmatlab/src/finiteElementHeatPropagator.c:688-739.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import prep
+
+
+def _distr(v):
+    return np.atleast_1d(np.asarray(v, dtype=np.float64)).reshape(1, -1)
+
+
+def prepare_mc(mdl, simType=1):
+    """Flat MEX-level inputs for one MC run (runMonteCarlo.m + getOpticalMediaProperties.m)."""
+    if simType != 1:
+        raise NotImplementedError("fluorescence MC (simType 2) is not supported by this host mirror")
+    G = mdl.G
+    MC = mdl.MC
+    if G.M_raw is None:
+        G.updateGeometry()
+    wl = np.atleast_1d(np.asarray(MC.wavelength, dtype=np.float64))
+    spectrum = np.array([float(MC.spectrumFunc(w)) for w in wl])
+    spectrum = spectrum / spectrum.sum()
+    DC = MC.depositionCriteria
+    if DC.onlyCollected and not DC.evaluateOnlyAtEndOfLife:
+        raise ValueError("Error: depositionCriteria.onlyCollected = true requires depositionCriteria.evaluateOnlyAtEndOfLife = true.")
+    if MC.nExamplePaths != 0 and wl.size != 1:
+        raise ValueError("Error: Example paths are not supported when simulating broadband illumination.")
+    if DC.onlyCollected and not MC.useLightCollector:
+        raise ValueError("Error: depositionCriteria.onlyCollected is true, but no light collector is defined")
+    if MC.farFieldRes and MC.boundaryType == 0:
+        raise ValueError("Error: If boundaryType == 0, no photons can escape to be registered in the far field. Set farFieldRes to zero or change boundaryType.")
+    if MC.useLightCollector and MC.boundaryType == 0:
+        raise ValueError("Error: If boundaryType == 0, no photons can escape to be registered on the light collector. Disable light collector or change boundaryType.")
+    media = G.mediaPropertiesFunc(G.mediaPropParams)
+    mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC)
+    SD = MC.sourceDistribution
+    if np.ndim(SD) == 0:
+        sd = None
+    else:
+        sd = np.asarray(SD, dtype=np.float32)
+        if sd.ndim == 3:
+            sd = sd[..., None]
+        if sd.shape != (G.nx, G.ny, G.nz, wl.size):
+            raise ValueError("Error: model.MC.sourceDistribution must be of size [nx, ny, nz, nLambda]")
+        if np.any(~np.isfinite(sd)) or np.any(sd < 0):
+            raise ValueError("Error: model.MC.sourceDistribution must be real, finite and non-negative")
+        # runMonteCarlo.m:65 normalises the distributed source to unit integral
+        sd = (sd / (G.dx * G.dy * G.dz * sd.sum(dtype=np.float64))).astype(np.float32)
+        sd = np.asfortranarray(sd)
+    LS = MC.lightSource
+    if sd is None and LS.sourceType in (3, 4, 5):
+        FP, AI = LS.FPID, LS.AID
+        if LS.sourceType == 3 and (math.isnan(FP.radialWidth) or math.isnan(AI.radialWidth)):
+            raise ValueError("Error: lightSource.focalPlaneIntensityDistribution.radialWidth and lightSource.angularIntensityDistribution.radialWidth must both be specified when sourceType is 3")
+        if LS.sourceType == 4 and (np.isnan(_distr(FP.radialDistr)[0, 0]) or np.isnan(_distr(AI.radialDistr)[0, 0])):
+            raise ValueError("Error: lightSource.focalPlaneIntensityDistribution.radialDistr and lightSource.angularIntensityDistribution.radialDistr must both be specified when sourceType is 4")
+        if LS.sourceType == 5 and (np.isnan(_distr(FP.XDistr)[0, 0]) or np.isnan(_distr(FP.YDistr)[0, 0])
+                                   or np.isnan(_distr(AI.XDistr)[0, 0]) or np.isnan(_distr(AI.YDistr)[0, 0])):
+            raise ValueError("Error: X and Y distributions must be specified when sourceType is 5")
+    LC = MC.lightCollector
+    if MC.useLightCollector:
+        if math.isfinite(LC.f):
+            xLCC = LC.x - LC.f * math.sin(LC.theta) * math.cos(LC.phi)
+            yLCC = LC.y - LC.f * math.sin(LC.theta) * math.sin(LC.phi)
+            zLCC = LC.z - LC.f * math.cos(LC.theta)
+        else:
+            xLCC, yLCC, zLCC = LC.x, LC.y, LC.z
+            if LC.res != 1:
+                raise ValueError("Error: lightCollector.res must be 1 when lightCollector.f is Inf")
+        if (abs(xLCC) < G.nx * G.dx / 2 and abs(yLCC) < G.ny * G.dy / 2 and abs(zLCC - G.nz * G.dz / 2) < G.nz * G.dz / 2):
+            raise ValueError("Error: Light collector center (%.4f,%.4f,%.4f) is inside cuboid" % (xLCC, yLCC, zLCC))
+    return dict(
+        nx=G.nx, ny=G.ny, nz=G.nz, dx=G.dx, dy=G.dy, dz=G.dz,
+        M=mp["M"], mua=mp["mua"], mus=mp["mus"], g=mp["g"], n=mp["n"], CDFidx=mp["CDFidx"],
+        CDFs=mp["CDFs"], interfaceNormals=mp["interfaceNormals"], sourceDistribution=sd,
+        spectrum=spectrum, wavelength=wl,
+        nPhotonsRequested=float(MC.nPhotonsRequested), simulationTimeRequested=float(MC.simulationTimeRequested),
+        requestCollectedPhotons=bool(MC.requestCollectedPhotons), calcNFR=bool(MC.calcNormalizedFluenceRate),
+        useLightCollector=bool(MC.useLightCollector), silentMode=True, useAllCPUs=bool(MC.useAllCPUs),
+        farFieldRes=int(MC.farFieldRes), boundaryType=int(MC.boundaryType), nExamplePaths=int(MC.nExamplePaths),
+        GPUdevice=int(MC.GPUdevice), seed=int(MC.seed),
+        LS=dict(sourceType=int(LS.sourceType), xFocus=float(LS.xFocus), yFocus=float(LS.yFocus), zFocus=float(LS.zFocus),
+                theta=float(LS.theta), phi=float(LS.phi), psi=float(LS.psi), emitterLength=float(LS.emitterLength),
+                FPID=dict(radialDistr=_distr(LS.FPID.radialDistr), radialWidth=float(LS.FPID.radialWidth),
+                          XDistr=_distr(LS.FPID.XDistr), XWidth=float(LS.FPID.XWidth),
+                          YDistr=_distr(LS.FPID.YDistr), YWidth=float(LS.FPID.YWidth)),
+                AID=dict(radialDistr=_distr(LS.AID.radialDistr), radialWidth=float(LS.AID.radialWidth),
+                         XDistr=_distr(LS.AID.XDistr), XWidth=float(LS.AID.XWidth),
+                         YDistr=_distr(LS.AID.YDistr), YWidth=float(LS.AID.YWidth))),
+        LC=dict(x=float(LC.x), y=float(LC.y), z=float(LC.z), theta=float(LC.theta), phi=float(LC.phi), f=float(LC.f),
+                diam=float(LC.diam), fieldSize=float(LC.fieldSize), NA=float(LC.NA), res=float(LC.res),
+                tStart=float(LC.tStart), tEnd=float(LC.tEnd), nTimeBins=float(LC.nTimeBins)),
+        DC=dict(minScatterings=float(DC.minScatterings), maxScatterings=float(DC.maxScatterings),
+                minRefractions=float(DC.minRefractions), maxRefractions=float(DC.maxRefractions),
+                minReflections=float(DC.minReflections), maxReflections=float(DC.maxReflections),
+                minInterfaceTransitions=float(DC.minInterfaceTransitions),
+                maxInterfaceTransitions=float(DC.maxInterfaceTransitions),
+                minSubmediaIdx=float(mp["minSubmediaIdx"]), maxSubmediaIdx=float(mp["maxSubmediaIdx"]),
+                onlyCollected=bool(DC.onlyCollected), evaluateOnlyAtEndOfLife=bool(DC.evaluateOnlyAtEndOfLife)),
+        mediaNames=mp["names"],
+    )
+
+
+def mex_model_tree(mc_in):
+    """Nested property tree of an MCmatlab.model as MCmatlab.c's mexFunction reads it."""
+    f32nan = np.array([[np.nan]], dtype=np.float32)
+    MC = dict(
+        silentMode=True, calcNFR=bool(mc_in["calcNFR"]),
+        LS=dict(mc_in["LS"]),
+        sourceDistribution=f32nan if mc_in["sourceDistribution"] is None else mc_in["sourceDistribution"],
+        nPhotonsRequested=mc_in["nPhotonsRequested"], simulationTimeRequested=mc_in["simulationTimeRequested"],
+        requestCollectedPhotons=mc_in["requestCollectedPhotons"],
+        mediaProperties=dict(mua=np.asfortranarray(mc_in["mua"]), mus=np.asfortranarray(mc_in["mus"]),
+                             g=np.asfortranarray(mc_in["g"]), n=np.asfortranarray(mc_in["n"]),
+                             CDFidx=np.asfortranarray(mc_in["CDFidx"])),
+        M=mc_in["M"], farFieldRes=float(mc_in["farFieldRes"]), boundaryType=float(mc_in["boundaryType"]),
+        interfaceNormals=f32nan if mc_in["interfaceNormals"] is None else mc_in["interfaceNormals"],
+        CDFs=np.asfortranarray(mc_in["CDFs"]) if np.size(mc_in["CDFs"]) else np.zeros((0, 0)),
+        depositionCriteria=dict(mc_in["DC"]), LC=dict(mc_in["LC"]),
+        useLightCollector=mc_in["useLightCollector"], nExamplePaths=float(mc_in["nExamplePaths"]),
+        spectrum=np.asarray(mc_in["spectrum"], dtype=np.float64).reshape(1, -1),
+        useAllCPUs=mc_in["useAllCPUs"], GPUdevice=float(mc_in["GPUdevice"]), seed=float(mc_in["seed"]),
+    )
+    G = dict(dx=float(mc_in["dx"]), dy=float(mc_in["dy"]), dz=float(mc_in["dz"]))
+    return dict(MC=MC, G=G, FMC=dict())
+
+
+def heat_mex_params(M1, A, E, c, dTdt_abs, useAllCPUs, heatBoundaryType, sensorIdx, sensorW,
+                    lightsOn, steps, dt):
+    """heatSimParameters as passed to finiteElementHeatPropagator (simulateHeatDistribution.m:209-211, :254-256)."""
+    nS = 0 if sensorIdx is None else len(sensorIdx)
+    return dict(
+        M=np.asfortranarray((M1.astype(np.int16) - 1).astype(np.uint8)),
+        A=np.asarray(A, dtype=np.float64).reshape(-1, 1),
+        E=np.asarray(E, dtype=np.float64).reshape(-1, 1),
+        dTdtperdeltaT=np.asfortranarray(np.asarray(c, dtype=np.float32)),
+        dTdt_abs=np.asfortranarray(np.asarray(dTdt_abs, dtype=np.float32)),
+        useAllCPUs=bool(useAllCPUs), heatBoundaryType=float(heatBoundaryType),
+        tempSensorCornerIdxs=(np.zeros((0, 0)) if nS == 0 else np.asarray(sensorIdx, dtype=np.float64).reshape(-1, 1)),
+        tempSensorInterpWeights=(np.zeros((0, 0)) if nS == 0 else np.asfortranarray(np.asarray(sensorW, dtype=np.float64))),
+        lightsOn=bool(lightsOn), steps=float(steps), dt=float(dt),
+    )

@@ -1,0 +1,344 @@
+"""Host-side input preparation for the two hot paths.
+
+The reference prepares the MEX inputs in MATLAB. MATLAB is not part of this
+library's runtime, so the preparation steps that feed the kernels are restated
+here in numpy, each citing the MATLAB function it follows:
+
+* geometry evaluation           +MCmatlab/@geometry/geometry.m:44-66, :130-138
+* optical media properties      +MCmatlab/@model/private/getOpticalMediaProperties.m:1-258
+* Sobel interface normals       +MCmatlab/@model/private/imgradientxyz.m:38-59 and
+                                getOpticalMediaProperties.m:222-244 (the branch without
+                                smoothn smoothing, :232-233)
+* thermal media properties      +MCmatlab/@model/private/getThermalMediaProperties.m
+* dT/dt arrays, dt limit        +MCmatlab/@model/simulateHeatDistribution.m:469-514
+* temperature sensor weights    +MCmatlab/@model/simulateHeatDistribution.m:543-609
+
+All arrays use MATLAB's column-major voxel order (x fastest): a grid array is a
+numpy array of shape (nx, ny, nz) in Fortran order, flattened with order="F".
+"""
+from __future__ import annotations
+
+import inspect
+import math
+
+import numpy as np
+
+CDFSIZE = 201  # +MCmatlab/src/MCmatlab.c:171 (one more than the 200 theta bins below)
+
+
+def _nargs(f):
+    try:
+        return len(inspect.signature(f).parameters)
+    except (TypeError, ValueError):
+        return 1
+
+
+def eval_optical(f, wavelength):
+    """Evaluates a medium property given as a number, f(wavelength) or f(wavelength, FR, T, FD).
+
+    The reference wraps numbers and one-argument functions into four-argument
+    functions (+MCmatlab/@mediumProperties/mediumProperties.m:30-52) and evaluates
+    them at (wavelength, 0, 0, 0) for media without FR/T/FD dependence
+    (getOpticalMediaProperties.m:72-92).
+    """
+    if callable(f):
+        n = _nargs(f)
+        return f(wavelength) if n == 1 else f(wavelength, 0.0, 0.0, 0.0)
+    return f
+
+
+def eval_thermal(f, T=37.0, FD=0.0):
+    """Thermal property given as a number or f(T, FD) (mediumProperties.m:180-207)."""
+    if callable(f):
+        return f(T, FD)
+    return f
+
+
+def geometry_axes(nx, ny, nz, Lx, Ly, Lz):
+    """Voxel-centre coordinates; x and y are centred on 0, z starts at 0 (geometry.m:121-138)."""
+    dx, dy, dz = Lx / nx, Ly / ny, Lz / nz
+    x = (np.arange(nx) - (nx - 1) / 2) * dx
+    y = (np.arange(ny) - (ny - 1) / 2) * dy
+    z = (np.arange(nz) + 0.5) * dz
+    return x, y, z
+
+
+def evaluate_geometry(G):
+    """Runs geomFunc on single-precision ndgrid coordinates (geometry.m:44-66)."""
+    x, y, z = geometry_axes(G.nx, G.ny, G.nz, G.Lx, G.Ly, G.Lz)
+    X, Y, Z = np.meshgrid(x.astype(np.float32), y.astype(np.float32), z.astype(np.float32), indexing="ij")
+    M = np.asarray(G.geomFunc(X, Y, Z, G.geomFuncParams))
+    if M.shape != (G.nx, G.ny, G.nz):
+        raise ValueError("Error: The M returned by the geometry function must be nx by ny by nz in size.")
+    if np.any(M <= 0):
+        raise ValueError("Error: The M returned by the geometry function must only contain positive numbers.")
+    if np.any(np.mod(M, 1)):
+        raise ValueError("Error: The M returned by the geometry function must only contain integers.")
+    if np.any(M > 255):
+        raise ValueError("Error: The M returned by the geometry function must not contain numbers over 255.")
+    return np.asfortranarray(M.astype(np.uint8))
+
+
+def _replicate_pad(I):
+    return np.pad(I, 1, mode="edge")
+
+
+def sobel_gradients(I):
+    """3D Sobel gradient with replicated borders (imgradientxyz.m 'sobel', correlation).
+
+    Returns (Gx, Gy, Gz) as derivatives along the first (x), second (y) and third (z)
+    array dimension. imgradientxyz names its outputs the other way round for the
+    first two (its 'Gx' differentiates along columns), which getOpticalMediaProperties.m:229
+    undoes by unpacking them as [Gy_Sobel, Gx_Sobel, Gz_Sobel].
+    """
+    I = np.asarray(I, dtype=np.float64)
+    P = _replicate_pad(I)
+    s = np.array([[1.0, 3.0, 1.0], [3.0, 6.0, 3.0], [1.0, 3.0, 1.0]])  # transverse weights
+    nx, ny, nz = I.shape
+
+    def sl(o0, o1, o2):
+        return P[1 + o0:1 + o0 + nx, 1 + o1:1 + o1 + ny, 1 + o2:1 + o2 + nz]
+
+    Gx = np.zeros_like(I)
+    Gy = np.zeros_like(I)
+    Gz = np.zeros_like(I)
+    for a in (-1, 0, 1):
+        for b in (-1, 0, 1):
+            # derivative along x: weights s over (y, z) offsets
+            w = s[a + 1, b + 1]
+            Gx += w * (sl(1, a, b) - sl(-1, a, b))
+            Gy += w * (sl(a, 1, b) - sl(a, -1, b))
+            Gz += w * (sl(a, b, 1) - sl(a, b, -1))
+    return Gx, Gy, Gz
+
+
+def interface_normals(M1, n_per_submedium, dx, dy, dz):
+    """(theta, phi) of the interface normal per voxel, float32 [2, L] (getOpticalMediaProperties.m:222-240).
+
+    M1 is the 1-based sub-medium grid; n_per_submedium is the [nSM, nL] refractive
+    index table. Voxels are grouped by unique refractive-index rows; for each group the
+    Sobel gradient of the group's indicator gives the normal inside that group.
+    """
+    nrows = np.asarray(n_per_submedium, dtype=np.float64)
+    if nrows.ndim == 1:
+        nrows = nrows[:, None]
+    uniq, inv = np.unique(nrows, axis=0, return_inverse=True)
+    inv = np.asarray(inv).reshape(-1)
+    ri_class = inv[M1.astype(np.int64) - 1]
+    Gx = np.full(M1.shape, np.nan)
+    Gy = np.full(M1.shape, np.nan)
+    Gz = np.full(M1.shape, np.nan)
+    for k in range(uniq.shape[0]):
+        mask = ri_class == k
+        gx, gy, gz = sobel_gradients(mask)
+        Gx[mask] = (gx / dx)[mask]
+        Gy[mask] = (gy / dy)[mask]
+        Gz[mask] = (gz / dz)[mask]
+    # cart2sph: phi = atan2(y, x), elevation = atan2(z, hypot(x, y)); theta = pi/2 - elevation
+    phi = np.arctan2(Gy, Gx)
+    elev = np.arctan2(Gz, np.hypot(Gx, Gy))
+    theta = np.pi / 2 - elev
+    out = np.empty((2, M1.size), dtype=np.float32)
+    out[0] = theta.reshape(-1, order="F")
+    out[1] = phi.reshape(-1, order="F")
+    return out
+
+
+def custom_phase_cdf(phase_func, wavelength):
+    """201-entry CDF of a custom phase function over 200 theta bins (getOpticalMediaProperties.m:94-102)."""
+    n_thetas = CDFSIZE - 1
+    thetas = np.pi / n_thetas * (np.arange(1, n_thetas + 1) - 0.5)
+    pdf = np.array([math.sin(t) * float(phase_func(wavelength, t)) for t in thetas])
+    if not np.all(np.isfinite(pdf)) or np.any(pdf < 0):
+        raise ValueError("Error: The custom phase function did not return real, finite, non-negative numbers.")
+    return np.concatenate([[0.0], np.cumsum(pdf) / np.sum(pdf)])
+
+
+def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC):
+    """Per-sub-medium optical tables and the sub-medium grid (getOpticalMediaProperties.m).
+
+    Media with FR/T/FD-dependent properties (nBins > 1, sub-media splitting) are not
+    supported by this preparation step; each medium maps to one sub-medium.
+    Returns a dict with mua, mus, g, n, CDFidx ([nSM, nL] float64), M (uint8, 1-based),
+    CDFs ([201, nCDF] float64), interfaceNormals (float32 [2, L] or None) and the
+    sub-media index range of the deposition criteria (1-based, may be inf).
+    """
+    wavelengths = np.atleast_1d(np.asarray(wavelengths, dtype=np.float64))
+    unique_media, M_trim = np.unique(M_raw, return_inverse=True)
+    M_trim = M_trim.reshape(M_raw.shape) + 1
+    trimmed = [mediaList[int(m) - 1] for m in unique_media]
+    names = [m.name for m in trimmed]
+    if len(set(names)) != len(names):
+        raise ValueError("Error: Two media have the same name.")
+    nM = len(trimmed)
+    nL = wavelengths.size
+    for m in trimmed:
+        if getattr(m, "nBins", 1) != 1:
+            raise NotImplementedError("sub-media splitting (nBins > 1) is not supported")
+    mua = np.full((nM, nL), np.nan)
+    mus = np.full((nM, nL), np.nan)
+    g = np.full((nM, nL), np.nan)
+    n = np.full((nM, nL), np.nan)
+    CDFidx = np.full((nM, nL), np.nan)
+    cdfs = []
+    minSub, maxSub = np.inf, np.inf
+    for iM, med in enumerate(trimmed):
+        for iL, L in enumerate(wavelengths):
+            a = float(np.float32(eval_optical(med.mua, L)))
+            s = float(np.float32(eval_optical(med.mus, L)))
+            gv = eval_optical(med.g, L)
+            gv = float(np.float32(gv)) if gv is not None else math.nan
+            if not math.isfinite(a):
+                raise ValueError("The mua function of medium %s returns NaN or Inf values." % med.name)
+            if not math.isfinite(s):
+                raise ValueError("The mus function of medium %s returns NaN or Inf values." % med.name)
+            if math.isfinite(gv):
+                g[iM, iL] = gv
+            else:
+                cdf = custom_phase_cdf(med.customPhaseFunc, L)
+                idx = None
+                for k, c in enumerate(cdfs):
+                    if np.array_equal(c, cdf):
+                        idx = k
+                        break
+                if idx is None:
+                    cdfs.append(cdf)
+                    idx = len(cdfs) - 1
+                CDFidx[iM, iL] = idx
+            mua[iM, iL] = a
+            mus[iM, iL] = s
+            n[iM, iL] = float(eval_optical(med.n, L))
+        if DC.minMediumIdxToConsider == unique_media[iM]:
+            minSub = iM + 1
+        if DC.maxMediumIdxToConsider == unique_media[iM]:
+            maxSub = iM + 1
+    if matchedInterfaces:
+        n[:] = 1.0
+    if np.any(~np.isfinite(mua)) or np.any(mua <= 0):
+        raise ValueError("Error: A medium has invalid mua. Must be finite, real and positive.")
+    if np.any(~np.isfinite(mus)) or np.any(mus <= 0):
+        raise ValueError("Error: A medium has invalid mus. Must be finite, real and positive.")
+    if not np.all(np.isnan(g) | (np.isfinite(g) & (np.abs(g) <= 1))):
+        raise ValueError("Error: A medium has invalid g. Must be finite, real and between -1 and 1, or NaN.")
+    if np.any(np.isnan(n)) or np.any(n < 1):
+        raise ValueError("Error: A medium has invalid n. Must not be NaN, must be real and at least 1.")
+    M = np.asfortranarray(M_trim.astype(np.uint8))
+    normals = None if matchedInterfaces else interface_normals(M, n, dx, dy, dz)
+    CDFs = np.stack(cdfs, axis=1) if cdfs else np.zeros((0, 0))
+    return dict(mua=mua, mus=mus, g=g, n=n, CDFidx=CDFidx, M=M, CDFs=CDFs,
+                interfaceNormals=normals, minSubmediaIdx=minSub, maxSubmediaIdx=maxSub,
+                names=names)
+
+
+def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0):
+    """VHC, TC, A, E per sub-medium and the sub-medium grid (getThermalMediaProperties.m).
+
+    Only temperature/damage-independent thermal properties are supported (nBins = 1).
+    """
+    unique_media, M_trim = np.unique(M_raw, return_inverse=True)
+    M_trim = M_trim.reshape(M_raw.shape) + 1
+    trimmed = [mediaList[int(m) - 1] for m in unique_media]
+    VHC = np.array([float(np.float32(eval_thermal(m.VHC, T, FD))) for m in trimmed])
+    TC = np.array([float(np.float32(eval_thermal(m.TC, T, FD))) for m in trimmed])
+    if np.any(~np.isfinite(VHC)) or np.any(VHC <= 0):
+        raise ValueError("The VHC function of a medium returns values that are not finite and positive.")
+    if np.any(~np.isfinite(TC)) or np.any(TC <= 0):
+        raise ValueError("The TC function of a medium returns values that are not finite and positive.")
+    A = np.array([float(m.A) for m in trimmed])
+    E = np.array([float(m.E) for m in trimmed])
+    return dict(VHC=VHC, TC=TC, A=A, E=E, M=np.asfortranarray(M_trim.astype(np.uint8)),
+                names=[m.name for m in trimmed])
+
+
+def calc_dTdt_arrays(VHC, TC, dx, dy, dz, NA_sum, P, M1):
+    """dTdtperdeltaT [nM, nM, 3] and dTdt_abs [L] in single precision (simulateHeatDistribution.m:469-494).
+
+    TC_eff(i, j) = 2 TC_i TC_j / (TC_i + TC_j); c(i, j, d) = TC_eff(i, j) / VHC_i / d_d^2;
+    dTdt_abs = NA * P / VHC(M). NA_sum is the normalised absorption summed over wavelengths.
+    """
+    VHC = np.asarray(VHC, dtype=np.float32)
+    TC = np.asarray(TC, dtype=np.float32)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        TC_eff = (2 * np.outer(TC, TC) / (TC[None, :] + TC[:, None])).astype(np.float32)
+    TC_eff[np.isnan(TC_eff)] = 0
+    rowv = VHC[:, None]
+    c = np.empty((len(VHC), len(VHC), 3), dtype=np.float32)
+    # MATLAB evaluates single-double mixtures in single precision
+    c[:, :, 0] = (TC_eff / rowv) / np.float32(dx ** 2)
+    c[:, :, 1] = (TC_eff / rowv) / np.float32(dy ** 2)
+    c[:, :, 2] = (TC_eff / rowv) / np.float32(dz ** 2)
+    NAP = (np.asarray(NA_sum, dtype=np.float64) * P).astype(np.float32)
+    dTdt_abs = NAP / VHC[M1.astype(np.int64) - 1]
+    return np.asfortranarray(c), np.asfortranarray(dTdt_abs)
+
+
+def calc_dtmax(M1, TC, VHC, dx, dy, dz):
+    """Smallest explicit-stability time step over all voxels (simulateHeatDistribution.m:496-514)."""
+    TCv = np.asarray(TC, dtype=np.float32)[M1.astype(np.int64) - 1]
+    VHCv = np.asarray(VHC, dtype=np.float32)[M1.astype(np.int64) - 1]
+    nx, ny, nz = M1.shape
+    ex = np.zeros((nx + 1, ny, nz), np.float32)
+    ey = np.zeros((nx, ny + 1, nz), np.float32)
+    ez = np.zeros((nx, ny, nz + 1), np.float32)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ex[1:-1] = 2 * TCv[:-1] * TCv[1:] / (TCv[:-1] + TCv[1:])
+        ey[:, 1:-1] = 2 * TCv[:, :-1] * TCv[:, 1:] / (TCv[:, :-1] + TCv[:, 1:])
+        ez[:, :, 1:-1] = 2 * TCv[:, :, :-1] * TCv[:, :, 1:] / (TCv[:, :, :-1] + TCv[:, :, 1:])
+    for e in (ex, ey, ez):
+        e[np.isnan(e)] = 0
+    fx, fy, fz = np.float32(dx ** 2), np.float32(dy ** 2), np.float32(dz ** 2)
+    denom = (ex[:-1] / fx + ex[1:] / fx + ey[:, :-1] / fy + ey[:, 1:] / fy
+             + ez[:, :, :-1] / fz + ez[:, :, 1:] / fz)
+    with np.errstate(divide="ignore"):
+        ind = VHCv / denom
+    return float(np.min(ind))
+
+
+def convert_temp_sensor_pos(positions, x, y, z):
+    """Corner voxel (0-based linear index) and interpolation weights of each sensor (simulateHeatDistribution.m:543-609)."""
+    positions = np.atleast_2d(np.asarray(positions, dtype=np.float64))
+    nS = positions.shape[0] if positions.size else 0
+    nx, ny, nz = len(x), len(y), len(z)
+    li = np.zeros(nS)
+    w = np.zeros((nS, 3))
+    axes = [(x, nx), (y, ny), (z, nz)]
+    for i in range(nS):
+        idx = []
+        for d, (ax, n) in enumerate(axes):
+            step = ax[1] - ax[0]
+            rel = positions[i, d] - ax[0]
+            if rel < 0:
+                k, wt = 0, 0.0
+            elif rel < ax[-1] - ax[0]:
+                k, wt = int(math.floor(rel / step)), math.fmod(rel / step, 1.0)
+            else:
+                k, wt = n - 2, 1.0
+            idx.append(k)
+            w[i, d] = wt
+        li[i] = idx[0] + idx[1] * nx + idx[2] * nx * ny
+    return li, w
+
+
+def heat_schedule(durationOn, durationOff, durationEnd, nUpdates, dtmax):
+    """Updates, steps per update and dt per phase (simulateHeatDistribution.m:80-110)."""
+    tot = durationOn + durationOff
+    out = {}
+    if durationOn != 0:
+        nU = max(1, round(nUpdates * durationOn / tot))
+        nT = math.ceil(durationOn / nU / dtmax)
+        out["on"] = (nU, nT, durationOn / nU / nT)
+    else:
+        out["on"] = (0, 1, 1.0)
+    if durationOff != 0:
+        nU = max(1, nUpdates - out["on"][0])
+        nT = math.ceil(durationOff / nU / dtmax)
+        out["off"] = (nU, nT, durationOff / nU / nT)
+    else:
+        out["off"] = (0, 1, 1.0)
+    if durationEnd != 0:
+        nU = max(1, round(nUpdates * durationEnd / tot))
+        nT = math.ceil(durationEnd / nU / dtmax)
+        out["end"] = (nU, nT, durationEnd / nU / nT)
+    else:
+        out["end"] = (0, 1, 1.0)
+    return out

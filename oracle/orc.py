@@ -1,0 +1,79 @@
+"""ctypes access to the FP64 CPU restatements in oracle/_ref/liboracle.so.
+
+TEST INFRASTRUCTURE ONLY (the checker): imported by tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg.
+
+  oracle_mc(mc_in, nthreads)             mc_oracle.c:orc_mc_run on MEX-level inputs
+  oracle_heat(T, Omega, heat_params)     heat_oracle.c:orc_heat_run (FP64 DG-ADI)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from mcmatlab_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "_ref", "liboracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError("oracle/_ref/liboracle.so is missing; run `make -C oracle oracle`")
+        L = C.CDLL(path)
+        L.orc_mc_run.argtypes = [C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_result), C.c_int]
+        L.orc_mc_run.restype = C.c_int
+        dp = C.POINTER(C.c_double)
+        L.orc_heat_run.argtypes = [C.c_long, C.c_long, C.c_long, C.c_int, C.POINTER(C.c_uint8), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), dp, dp, C.c_int, C.c_int, C.c_long, C.c_double,
+                                   dp, dp, C.c_int, dp, dp, dp, dp]
+        L.orc_heat_run.restype = C.c_int
+        L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.orc_lambert_wm1.argtypes = [C.c_double]
+        L.orc_lambert_wm1.restype = C.c_double
+        for f in ("orc_sizeof_mc_model", "orc_sizeof_mc_result", "orc_sizeof_heat_params"):
+            getattr(L, f).restype = C.c_size_t
+        _LIB = L
+    return _LIB
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().orc_philox(c, k, o)
+    return list(o)
+
+
+def oracle_mc(mc_in, nthreads=0):
+    mb = abi.McModelBuffers(mc_in)
+    rb = abi.McResultBuffers(mc_in)
+    rc = lib().orc_mc_run(C.byref(mb.model), C.byref(rb.result), int(nthreads))
+    if rc != 0:
+        raise RuntimeError("oracle MC run failed (%d)" % rc)
+    return rb.outputs()
+
+
+def oracle_heat(T, Omega, hp, nx, ny, nz):
+    """FP64 DG-ADI over hp['steps'] steps. Returns (T, Omega or None, sensorTemps [nS, nt+1], maxMediaTemps)."""
+    hb = abi.HeatParamBuffers(nx, ny, nz, hp)
+    p = hb.params
+    Td = np.ascontiguousarray(np.asarray(T, dtype=np.float64).reshape(-1, order="F"))
+    Od = None if Omega is None else np.ascontiguousarray(np.asarray(Omega, dtype=np.float64).reshape(-1, order="F"))
+    nt = int(p.steps)
+    sens = np.zeros(hb.nS * (nt + 1)) if hb.nS else None
+    mx = np.zeros(hb.nM)
+    dp = C.POINTER(C.c_double)
+    nul = C.cast(None, dp)
+    lib().orc_heat_run(nx, ny, nz, hb.nM, p.M, p.dTdtperdeltaT, p.dTdt_abs, p.A, p.E, p.lightsOn, p.heatBoundaryType,
+                       nt, p.dt, Td.ctypes.data_as(dp), Od.ctypes.data_as(dp) if Od is not None else nul, hb.nS,
+                       p.tempSensorCornerIdxs, p.tempSensorInterpWeights,
+                       sens.ctypes.data_as(dp) if sens is not None else nul, mx.ctypes.data_as(dp))
+    shp = (nx, ny, nz)
+    return (Td.reshape(shp, order="F"), None if Od is None else Od.reshape(shp, order="F"),
+            None if sens is None else sens.reshape(hb.nS, nt + 1, order="F"), mx)
