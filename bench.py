@@ -1,0 +1,313 @@
+"""Benchmark: coupled heat simulation on the standard-tissue cube (the C0 geometry), plus the
+plain MC transport of that cube, on B200 through the library's C ABI.
+
+Workload ("coupled heat on config-0 geometry"):
+  * geometry: 100^3 voxels over a 0.1 cm cube (air / epidermis / dermis / vessel);
+  * heat source: absorbed power of a 1 W pencil beam from a 1e6-packet MC run (seed 1);
+  * thermal: VHC 3.9, TC 0.0037 (tissue), VHC 0.0012, TC 0.00026 (air); T0 = 37 degC;
+    damage in the vessel (E = 4.48e5 J/mol, A = 7.6e66 /s); insulating faces;
+  * dt = 0.9 x the explicit stability limit (calcdtmax);
+  * one bench step = one call of the stepper over `--nt` DG-ADI time steps with the light on
+    (the illumination phase of the schedule; a full update call of that phase is ~1.45e5 steps).
+Metric: heat voxel-updates/s (voxels x time steps / s), whole job. The MC transport of the
+same cube (photon packets/s) is reported in the same line under "mc".
+
+Timing: `value` = device time (CUDA events recorded by the library on its own stream) of the
+stepping loop with all grids resident in HBM; L2 is flushed (256 MB write) between timed steps
+because the 100^3 working set (~30 MB) is smaller than L2. `e2e` = the same metric through
+mcb_heat_forward with host buffers (H2D of the inputs and D2H of T, Omega, sensors and maxima
+inside the timed region), wall clock per call.
+
+`--impl reference` times the reference's own C heat stepper (finiteElementHeatPropagator.c,
+compiled from source with the reference's flags into oracle/_ref) on all host cores, on a
+bounded sample of steps of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from mcmatlab_b200 import configs, mexargs, prep  # noqa: E402
+
+METRIC = "photon packets/s, heat voxel-updates/s on 1 B200; batched+adjoint vs plain"
+N_GRID = 100
+MC_PACKETS = 1_000_000
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_heat_inputs(NA_sum, m):
+    G = m.G
+    media = G.mediaPropertiesFunc([])
+    th = prep.thermal_media_properties(media, G.M_raw)
+    c, Q = prep.calc_dTdt_arrays(th["VHC"], th["TC"], G.dx, G.dy, G.dz, NA_sum, 1.0, th["M"])
+    dtmax = prep.calc_dtmax(th["M"], th["TC"], th["VHC"], G.dx, G.dy, G.dz)
+    dt = 0.9 * dtmax
+    return th, c, Q, dt
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index=0):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            sm = [float(r[1]) for r in rows]
+            mx = float(rows[0][2])
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for k, nme in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(nme)
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, ws, dist
+
+
+def run_ours(args):
+    import torch
+    from mcmatlab_b200 import native
+    rank, ws, dist = dist_init()
+    dev = torch.cuda.current_device() if torch.cuda.is_available() else 0
+    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=MC_PACKETS, seed=1 + rank)
+    mc_in = mexargs.prepare_mc(m)
+    # warm the transport once, then time it (packets/s on the cube)
+    mc_small = dict(mc_in)
+    mc_small["nPhotonsRequested"] = 1e5
+    native.mc_run(mc_small, device=dev)
+    t0 = time.perf_counter()
+    out = native.mc_run(mc_in, device=dev)
+    mc_wall = time.perf_counter() - t0
+    mc_ms = out["kernelMs"]
+    steps_mc = out["propagationSteps"]
+    NFR = out["NFR"][..., 0]
+    mua = mc_in["mua"][:, 0]
+    NA = mua[mc_in["M"].astype(np.int64) - 1].astype(np.float32) * NFR
+    th, c, Q, dt = build_heat_inputs(NA, m)
+    hp = mexargs.heat_mex_params(th["M"], th["A"], th["E"], c, Q, True, 0, None, None, True, args.nt, dt)
+    T0 = np.full((N_GRID,) * 3, 37.0, np.float32, order="F")
+    O0 = np.zeros((N_GRID,) * 3, np.float32, order="F")
+    L = N_GRID ** 3
+    state = native.HeatState(T0, O0, hp, N_GRID, N_GRID, N_GRID, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    for _ in range(args.warmup):
+        state.step(hp)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            state.step(hp)
+            times.append(native.last_kernel_ms(dev))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    dev_ms = float(sum(times))
+    # e2e through the host-buffer entry point
+    e2e_times = []
+    Tn, On = T0.copy(order="F"), O0.copy(order="F")
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        Tn, On, _, _ = native.heat_forward(Tn, On, hp, N_GRID, N_GRID, N_GRID, device=dev)
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(sum(e2e_times))
+    if dist:
+        t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, e2e_s = float(t[0]), float(t[1])
+    updates = float(L) * args.nt * args.steps * ws
+    value = updates / (dev_ms / 1e3)
+    e2e_value = updates / e2e_s
+    ms_per_step = dev_ms / args.steps
+    # roofline: algorithmic bytes per voxel-update with the light on: T read + write (8), M (1),
+    # source (4), plus Omega read + write (8) in the voxels that accumulate damage
+    frac_dmg = float(np.mean(th["E"][th["M"].astype(np.int64) - 1] != 0))
+    bytes_per_update = 9.0 + 4.0 + 8.0 * frac_dmg
+    hbm, src = peaks()
+    achieved = bytes_per_update * L * args.nt / (ms_per_step / 1e3) / 1e9
+    # one bench step: 3 passes per time step + the maxima decode
+    launches = args.steps * (3 * args.nt + 1)
+    res = {
+        "metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (tallies f64)", "data": "synthetic",
+        "config": {"workload": "coupled heat on the 100^3 standard-tissue cube (config-0 geometry), light on, "
+                               "DG-ADI + Arrhenius, dt = 0.9 x stability limit",
+                   "grid": [N_GRID] * 3, "time_steps_per_bench_step": args.nt, "dt_s": dt,
+                   "heat_source": "absorbed power of a 1e6-packet pencil-beam MC run at 1 W",
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": "replicas" if ws > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": "voxel-updates/s",
+                "h2d_bytes_per_step": int(L * (4 + 4 + 1 + 4) + 12 * len(th["VHC"]) ** 2 + 16 * len(th["VHC"])),
+                "d2h_bytes_per_step": int(L * 8 + 4 * len(th["VHC"])),
+                "timing": "wall clock around mcb_heat_forward (host buffers)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": src, "traffic": None,
+                     "algorithmic_bytes_per_voxel_update": bytes_per_update,
+                     "kernel": "DG-ADI step (pass_x + pass_yz<y> + pass_yz<z>)"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "mc": {"metric": "photon packets/s", "workload": "standard-tissue cube 100^3, pencil beam, 1e6 packets",
+               "value": MC_PACKETS / (mc_ms / 1e3), "e2e_value": MC_PACKETS / mc_wall,
+               "kernel_ms": mc_ms, "propagation_steps": steps_mc,
+               "steps_per_s": steps_mc / (mc_ms / 1e3)},
+    }
+    if rank == 0:
+        if args.cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
+        print(json.dumps(res), flush=True)
+    state.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_setup():
+    from oracle import ref
+    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=1e5, seed=1)
+    mc_in = mexargs.prepare_mc(m)
+    tree = mexargs.mex_model_tree(mc_in)
+    out = ref.RefMC().run(tree, seed=None)  # reference MC, all cores, for the heat source
+    NFR = out["NFR"]
+    NFR = NFR[..., 0] if NFR.ndim == 4 else NFR
+    mua = mc_in["mua"][:, 0]
+    NA = mua[mc_in["M"].astype(np.int64) - 1].astype(np.float32) * NFR
+    return m, NA
+
+
+def cpu_baseline(args, sample_steps):
+    """The reference's own heat stepper on all host cores, bounded sample of `sample_steps` steps."""
+    from oracle import ref
+    m, NA = reference_setup()
+    th, c, Q, dt = build_heat_inputs(NA, m)
+    hp = mexargs.heat_mex_params(th["M"], th["A"], th["E"], c, Q, True, 0, None, None, True, sample_steps, dt)
+    T0 = np.full((N_GRID,) * 3, 37.0, np.float32, order="F")
+    O0 = np.zeros((N_GRID,) * 3, np.float32, order="F")
+    R = ref.RefHeat()
+    cores = os.cpu_count()
+    R.run(T0, O0, dict(hp, steps=2.0), nthreads=cores)
+    t0 = time.perf_counter()
+    R.run(T0, O0, hp, nthreads=cores)
+    dtw = time.perf_counter() - t0
+    return {"value": N_GRID ** 3 * sample_steps / dtw, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
+            "sample": "%d DG-ADI steps of the same 100^3 workload (light on, damage), reference MEX C code "
+                      "(-Ofast -fopenmp) on %d host threads" % (sample_steps, cores)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref
+    m, NA = reference_setup()
+    th, c, Q, dt = build_heat_inputs(NA, m)
+    hp = mexargs.heat_mex_params(th["M"], th["A"], th["E"], c, Q, True, 0, None, None, True, args.ref_nt, dt)
+    T0 = np.full((N_GRID,) * 3, 37.0, np.float32, order="F")
+    O0 = np.zeros((N_GRID,) * 3, np.float32, order="F")
+    R = ref.RefHeat()
+    cores = os.cpu_count()
+    T, O = T0, O0
+    for _ in range(args.warmup):
+        T, O, _, _ = R.run(T, O, hp, nthreads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        T, O, _, _ = R.run(T, O, hp, nthreads=cores)
+        times.append(time.perf_counter() - t0)
+    tot = float(sum(times))
+    value = N_GRID ** 3 * args.ref_nt * args.steps / tot
+    res = {"metric": METRIC, "value": value, "unit": "voxel-updates/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": "coupled heat on the 100^3 standard-tissue cube (config-0 geometry), light on, "
+                                  "DG-ADI + Arrhenius, dt = 0.9 x stability limit",
+                      "grid": [N_GRID] * 3, "time_steps_per_bench_step": args.ref_nt, "dt_s": dt},
+           "cpu_baseline": {"value": value, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
+                            "sample": "%d DG-ADI steps per bench step" % args.ref_nt},
+           "e2e": {"value": value, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nt", type=int, default=20000, help="DG-ADI time steps per bench step")
+    ap.add_argument("--ref-nt", type=int, default=50, help="time steps per bench step of the CPU reference")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -25,6 +25,12 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#if defined(__GNUC__)
+#define MCB_API __attribute__((visibility("default")))
+#else
+#define MCB_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -42,12 +48,12 @@ typedef enum {
 typedef struct mcb_ctx mcb_ctx;
 
 /* One context per device and caller thread; it owns device buffers reused across calls. */
-mcb_status mcb_ctx_create(int device, mcb_ctx **out);
-mcb_status mcb_ctx_destroy(mcb_ctx *ctx);
-const char *mcb_last_error(const mcb_ctx *ctx);
+MCB_API mcb_status mcb_ctx_create(int device, mcb_ctx **out);
+MCB_API mcb_status mcb_ctx_destroy(mcb_ctx *ctx);
+MCB_API const char *mcb_last_error(const mcb_ctx *ctx);
 /* Host-visible cancel flag polled by the transport kernel (stands in for utIsInterruptPending,
  * MCmatlab.c:293-298). Setting *flag != 0 makes the running mcb_mc_run return MCB_ECANCELLED. */
-volatile int *mcb_cancel_flag(mcb_ctx *ctx);
+MCB_API volatile int *mcb_cancel_flag(mcb_ctx *ctx);
 
 /* ------------------------------------------------------------------------------------------
  * Monte Carlo photon transport.
@@ -117,12 +123,12 @@ typedef struct mcb_mc_result {
 } mcb_mc_result;
 
 /* Replaces MCmatlab.c mexFunction: runs all wavelengths, normalises and writes the outputs. */
-mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_result *result);
+MCB_API mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_result *result);
 
 /* No counterpart in the reference: runs n independent models (different grids, media,
  * wavelengths, photon counts) in one persistent launch. Results equal n calls of mcb_mc_run
  * up to FP64 summation order. */
-mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,
+MCB_API mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,
                             mcb_mc_result *const *results);
 
 /* ------------------------------------------------------------------------------------------
@@ -150,8 +156,24 @@ typedef struct mcb_heat_params {
  *   Omega        in/out [nx*ny*nz], or NULL for no damage (the MEX's NaN-scalar Omega)
  *   sensorTemps  out [nSensors x (steps+1)] (may be NULL when nSensors == 0)
  *   maxMediaTemps out [nM]: max over all voxels of medium m and all steps of T (-inf if none) */
-mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
+MCB_API mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
                             double *sensorTemps, float *maxMediaTemps);
+
+/* No counterpart in the reference (whose MEX re-uploads every grid on each call,
+ * finiteElementHeatPropagator.c:750, :811): a device-resident stepper state. The grids stay in
+ * HBM between calls of mcb_heat_state_step, which runs p->steps steps with p's lightsOn, dt,
+ * heatBoundaryType and sensors (p's grid and media must match the state's). */
+typedef struct mcb_heat_state mcb_heat_state;
+MCB_API mcb_status mcb_heat_state_create(mcb_ctx *ctx, const mcb_heat_params *p, const float *T, const float *Omega,
+                                         mcb_heat_state **out);
+MCB_API mcb_status mcb_heat_state_step(mcb_heat_state *state, const mcb_heat_params *p, double *sensorTemps,
+                                       float *maxMediaTemps);
+MCB_API mcb_status mcb_heat_state_read(mcb_heat_state *state, float *T, float *Omega);
+MCB_API mcb_status mcb_heat_state_destroy(mcb_heat_state *state);
+
+/* No counterpart in the reference: device time in milliseconds (CUDA events on the context's
+ * stream) of the transport kernel or stepping loop of the last call on this context. */
+MCB_API double mcb_last_kernel_ms(const mcb_ctx *ctx);
 
 #ifdef __cplusplus
 }

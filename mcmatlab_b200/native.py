@@ -1,0 +1,174 @@
+"""ctypes binding to the in-tree sm_100a library libmcb200.so (include/mcb200.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import threading
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmcb200.so")
+
+_lock = threading.Lock()
+_lib = None
+_ctx = {}
+
+STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB_ECANCELLED", 5: "MCB_ETIMEOUT",
+          6: "MCB_ELAUNCH"}
+
+EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
+           "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
+           "mcb_heat_state_destroy", "mcb_last_kernel_ms")
+
+
+class MCBError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+def lib():
+    """Loads libmcb200.so (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise FileNotFoundError("%s is missing: build it with `python -m mcmatlab_b200.build`" % LIB_PATH)
+            L = C.CDLL(LIB_PATH)
+            L.mcb_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+            L.mcb_ctx_destroy.argtypes = [C.c_void_p]
+            L.mcb_last_error.argtypes = [C.c_void_p]
+            L.mcb_last_error.restype = C.c_char_p
+            L.mcb_cancel_flag.argtypes = [C.c_void_p]
+            L.mcb_cancel_flag.restype = C.POINTER(C.c_int)
+            L.mcb_mc_run.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_result)]
+            L.mcb_mc_run_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.POINTER(abi.mcb_mc_model)),
+                                           C.POINTER(C.POINTER(abi.mcb_mc_result))]
+            L.mcb_heat_forward.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
+                                           C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
+            L.mcb_heat_state_create.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
+                                                C.POINTER(C.c_float), C.POINTER(C.c_void_p)]
+            L.mcb_heat_state_step.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_double),
+                                              C.POINTER(C.c_float)]
+            L.mcb_heat_state_read.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+            L.mcb_heat_state_destroy.argtypes = [C.c_void_p]
+            L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
+            L.mcb_last_kernel_ms.restype = C.c_double
+            _lib = L
+        return _lib
+
+
+def context(device=0):
+    with _lock:
+        if device not in _ctx:
+            L = lib() if _lib is None else _lib
+            p = C.c_void_p()
+            st = L.mcb_ctx_create(int(device), C.byref(p))
+            if st != 0:
+                raise MCBError(st, "could not create a context on CUDA device %d" % device)
+            _ctx[device] = p
+        return _ctx[device]
+
+
+def _check(st, ctx):
+    if st != 0:
+        raise MCBError(st, lib().mcb_last_error(ctx).decode())
+
+
+def mc_run(mc_in, device=0, example_cap=100000):
+    """Runs one model (MEX-level inputs from mexargs.prepare_mc); returns outputs in MATLAB shapes."""
+    ctx = context(device)
+    mb = abi.McModelBuffers(mc_in)
+    rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0)
+    _check(lib().mcb_mc_run(ctx, C.byref(mb.model), C.byref(rb.result)), ctx)
+    return rb.outputs()
+
+
+def mc_run_batch(mc_ins, device=0):
+    """Runs several models in one persistent launch; returns a list of output dicts."""
+    ctx = context(device)
+    mbs = [abi.McModelBuffers(x) for x in mc_ins]
+    rbs = [abi.McResultBuffers(x) for x in mc_ins]
+    n = len(mc_ins)
+    mp = (C.POINTER(abi.mcb_mc_model) * n)(*[C.pointer(m.model) for m in mbs])
+    rp = (C.POINTER(abi.mcb_mc_result) * n)(*[C.pointer(r.result) for r in rbs])
+    _check(lib().mcb_mc_run_batch(ctx, n, mp, rp), ctx)
+    return [r.outputs() for r in rbs]
+
+
+def heat_forward(T, Omega, hp, nx, ny, nz, device=0):
+    """finiteElementHeatPropagator equivalent. Omega None = no damage.
+    Returns (T, Omega or None, sensorTemps [nS, nt+1] or empty, maxMediaTemps [1, nM])."""
+    ctx = context(device)
+    hb = abi.HeatParamBuffers(nx, ny, nz, hp)
+    Tb = np.ascontiguousarray(np.asarray(T, dtype=np.float32).reshape(-1, order="F")).copy()
+    Ob = None if Omega is None else np.ascontiguousarray(np.asarray(Omega, dtype=np.float32).reshape(-1, order="F")).copy()
+    nt = int(hb.params.steps)
+    sens = np.zeros(hb.nS * (nt + 1)) if hb.nS else np.zeros(1)
+    mx = np.zeros(hb.nM, dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    _check(lib().mcb_heat_forward(ctx, C.byref(hb.params), Tb.ctypes.data_as(fp),
+                                  Ob.ctypes.data_as(fp) if Ob is not None else C.cast(None, fp),
+                                  sens.ctypes.data_as(C.POINTER(C.c_double)), mx.ctypes.data_as(fp)), ctx)
+    shp = (nx, ny, nz)
+    return (Tb.reshape(shp, order="F"), None if Ob is None else Ob.reshape(shp, order="F"),
+            sens.reshape(hb.nS, nt + 1, order="F") if hb.nS else np.zeros((0, 0)), mx.reshape(1, -1))
+
+
+def last_kernel_ms(device=0):
+    """Device time (CUDA events on the library's stream) of the last transport/stepping loop."""
+    return lib().mcb_last_kernel_ms(context(device))
+
+
+class HeatState:
+    """Device-resident heat stepper state (mcb_heat_state_*): grids stay in HBM between step() calls."""
+
+    def __init__(self, T, Omega, hp, nx, ny, nz, device=0):
+        self.ctx = context(device)
+        self.shape = (nx, ny, nz)
+        self.hb = abi.HeatParamBuffers(nx, ny, nz, hp)
+        self.damage = Omega is not None
+        Tb = np.ascontiguousarray(np.asarray(T, dtype=np.float32).reshape(-1, order="F"))
+        Ob = None if Omega is None else np.ascontiguousarray(np.asarray(Omega, dtype=np.float32).reshape(-1, order="F"))
+        fp = C.POINTER(C.c_float)
+        p = C.c_void_p()
+        _check(lib().mcb_heat_state_create(self.ctx, C.byref(self.hb.params), Tb.ctypes.data_as(fp),
+                                           Ob.ctypes.data_as(fp) if Ob is not None else C.cast(None, fp), C.byref(p)),
+               self.ctx)
+        self.ptr = p
+
+    def step(self, hp):
+        hb = abi.HeatParamBuffers(*self.shape, hp)
+        nt = int(hb.params.steps)
+        sens = np.zeros(max(hb.nS * (nt + 1), 1))
+        mx = np.zeros(hb.nM, dtype=np.float32)
+        _check(lib().mcb_heat_state_step(self.ptr, C.byref(hb.params), sens.ctypes.data_as(C.POINTER(C.c_double)),
+                                         mx.ctypes.data_as(C.POINTER(C.c_float))), self.ctx)
+        return (sens[:hb.nS * (nt + 1)].reshape(hb.nS, nt + 1, order="F") if hb.nS else np.zeros((0, 0))), mx.reshape(1, -1)
+
+    def read(self):
+        n = int(np.prod(self.shape))
+        T = np.zeros(n, dtype=np.float32)
+        O = np.zeros(n, dtype=np.float32) if self.damage else None
+        fp = C.POINTER(C.c_float)
+        _check(lib().mcb_heat_state_read(self.ptr, T.ctypes.data_as(fp), O.ctypes.data_as(fp) if O is not None else
+                                         C.cast(None, fp)), self.ctx)
+        return T.reshape(self.shape, order="F"), (None if O is None else O.reshape(self.shape, order="F"))
+
+    def close(self):
+        if self.ptr:
+            lib().mcb_heat_state_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,91 @@
+"""GPU transport parity: the CUDA kernel through the C ABI against the reference's own
+batches (golden) and against the FP64 CPU oracle on the same Philox streams."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import mccases
+import mcstats
+from mcmatlab_b200 import mexargs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+K = 8
+
+
+def gpu_batches(mc_in, K=K, first_seed=1):
+    from mcmatlab_b200 import native
+    out = []
+    for s in range(K):
+        mc_in["seed"] = first_seed + s
+        out.append(mcstats.summaries(native.mc_run(mc_in), mc_in))
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(mccases.CASES))
+def test_gpu_matches_reference_golden(name):
+    with open(os.path.join(GOLD, "mc_ref_summaries.json")) as f:
+        golden = json.load(f)[name]
+    mc_in = mexargs.prepare_mc(mccases.CASES[name]())
+    ok, rep, worst = mcstats.ztest(golden, gpu_batches(mc_in))
+    assert ok, rep
+
+
+@pytest.mark.parametrize("name", ["c0_small", "radial_lens_ff", "xy_custom_fiber_cyclic", "dc_end_of_life"])
+def test_gpu_matches_oracle_same_streams(name, oracle_lib):
+    from oracle import orc
+    mc_in = mexargs.prepare_mc(mccases.CASES[name]())
+    ob = []
+    for s in range(K):
+        mc_in["seed"] = 1 + s
+        ob.append(mcstats.summaries(orc.oracle_mc(mc_in, 0), mc_in))
+    ok, rep, worst = mcstats.ztest(ob, gpu_batches(mc_in))
+    assert ok, rep
+
+
+def test_gpu_deterministic_counters():
+    from mcmatlab_b200 import native
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    a = native.mc_run(mc_in)
+    b = native.mc_run(mc_in)
+    assert a["propagationSteps"] == b["propagationSteps"] and a["nPhotons"] == b["nPhotons"]
+    np.testing.assert_allclose(a["NFR"], b["NFR"], rtol=1e-9, atol=1e-12 * float(np.max(a["NFR"])))
+
+
+def test_gpu_energy_balance_c0():
+    """Absorbed + escaped weight = launched weight up to roulette noise (standard tissue cube)."""
+    from mcmatlab_b200 import native
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    mc_in["nPhotonsRequested"] = 2e5
+    o = native.mc_run(mc_in)
+    s = mcstats.summaries(o, mc_in)
+    absorbed = sum(v for k, v in s.items() if k.startswith("abs_m"))
+    escaped = sum(v for k, v in s.items() if k.startswith("NI_"))
+    assert abs(absorbed + escaped - 1.0) < 0.01, (absorbed, escaped)
+
+
+def test_gpu_requested_collected_and_timed_modes():
+    from mcmatlab_b200 import native
+    mc_in = mexargs.prepare_mc(mccases.xy_custom_fiber_cyclic())
+    mc_in["requestCollectedPhotons"] = True
+    mc_in["nPhotonsRequested"] = 500.0
+    o = native.mc_run(mc_in)
+    assert o["nPhotonsCollected"] >= 500 and o["nPhotons"] > o["nPhotonsCollected"]
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    mc_in["nPhotonsRequested"] = float("nan")
+    mc_in["simulationTimeRequested"] = 0.5 / 60  # half a second
+    o = native.mc_run(mc_in)
+    assert o["nPhotons"] > 1000 and 0.3 / 60 < o["simulationTime"] < 5.0 / 60
+
+
+def test_gpu_example_paths():
+    from mcmatlab_b200 import native
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    mc_in["nExamplePaths"] = 5
+    o = native.mc_run(mc_in)
+    P = o["examplePaths"]
+    assert P.shape[0] == 4 and P.shape[1] > 10
+    starts = np.sum(np.isnan(P[0, :-1]) & np.isnan(P[0, 1:]))
+    assert starts == 5
