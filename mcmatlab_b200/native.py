@@ -16,7 +16,7 @@ from . import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmcb200.so")
 
-_lock = threading.Lock()
+_lock = threading.RLock()
 _lib = None
 _ctx = {}
 
@@ -66,9 +66,9 @@ def lib():
 
 
 def context(device=0):
+    L = lib()
     with _lock:
         if device not in _ctx:
-            L = lib() if _lib is None else _lib
             p = C.c_void_p()
             st = L.mcb_ctx_create(int(device), C.byref(p))
             if st != 0:

@@ -36,3 +36,14 @@ def test_context_create_fails_cleanly_without_gpu():
     p = C.c_void_p()
     st = L.mcb_ctx_create(0, C.byref(p))
     assert st in (1, 3)  # MCB_EINVAL / MCB_ECUDA, never a crash
+
+
+def test_python_context_raises_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from mcmatlab_b200 import native
+    with pytest.raises(native.MCBError):
+        native.context(0)
+    with pytest.raises(native.MCBError):
+        native.context(0)
