@@ -39,6 +39,7 @@ struct HeatDev {
   const float *Q;  // dTdt_abs or nullptr when the light is off
   const float *ib; // [3][L] inverse pivots
   float *Omega;    // or nullptr
+  float *dOmega;   // damage accumulated during the current call, or nullptr
   const double *logA, *E;  // [nM]
   unsigned int *maxEnc;    // [nM] order-preserving encoded running maxima
   int hs;          // heat-sinked faces
@@ -79,39 +80,28 @@ __device__ void record_sensors(const HeatDev &h, int col) {
   }
 }
 
-// Line coefficients in the form used by the solver: a = dt/2 c(M_i, M_prev), cc = dt/2 c(M_i, M_next),
-// both zero at the line ends and for heat-sinked voxels (whose rows are identity rows).
-struct LineView {
-  const uint8_t *M;  // shared-memory line of medium indices
-  int stride;        // element stride of M in shared memory
-  int fstride;       // element stride of the float lines (rhs, pivots) in shared memory
-  int n;
-  bool lineSinked;   // whole line lies on a heat-sinked face
-  bool hs;
-  int dir;
-};
-
-__device__ __forceinline__ float coef_prev(const HeatDev &h, const LineView &L, int i) {
-  if (i == 0 || L.lineSinked || (L.hs && i == L.n - 1)) return 0.f;
-  return h.hdt * cf(h, L.M[i * L.stride], L.M[(i - 1) * L.stride], L.dir);
-}
-__device__ __forceinline__ float coef_next(const HeatDev &h, const LineView &L, int i) {
-  if (i == L.n - 1 || L.lineSinked || (L.hs && i == 0)) return 0.f;
-  return h.hdt * cf(h, L.M[i * L.stride], L.M[(i + 1) * L.stride], L.dir);
+// Tridiagonal line coefficients: a = dt/2 c(M_i, M_prev) couples a row to its predecessor,
+// cc = dt/2 c(M_i, M_next) to its successor; both vanish at the line ends and on heat-sinked
+// rows (identity rows), which reproduces the reference's heat-sink exceptions (:334-349).
+__device__ __forceinline__ bool row_sinked(const HeatDev &h, bool lineSinked, int i, int n) {
+  return lineSinked || (h.hs && (i == 0 || i == n - 1));
 }
 
-// Solves one tridiagonal line held in shared memory with one warp: rhs[i*st] is replaced by
-// the solution. Thomas forward sweep d'_i = rhs_i + (a_i * ib_{i-1}) d'_{i-1} and back
-// substitution T_i = ib_i d'_i + (cc_i ib_i) T_{i+1}, each evaluated as a chunked warp scan
-// of affine maps.
-__device__ void warp_solve(const HeatDev &h, const LineView &L, float *rhs, const float *ib) {
+// Solves one tridiagonal line with one warp. Shared-memory inputs (element stride st):
+//   rhs  right-hand side, replaced by the solution
+//   fm   forward multipliers  a_i / b'_{i-1}      (Thomas elimination d'_i = rhs_i + fm_i d'_{i-1})
+//   bm   backward multipliers cc_i / b'_i         (back substitution T_i = d'_i / b'_i + bm_i T_{i+1})
+//   ib   inverse pivots 1 / b'_i
+// Each recurrence is evaluated as a chunked warp scan of affine maps: every lane composes the
+// map of its contiguous chunk, a 5-step shuffle scan combines the lanes, and each lane then
+// replays its chunk from the carried-in value.
+__device__ void warp_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
   const int lane = threadIdx.x & 31;
-  const int n = L.n, st = L.fstride;
   const int k = (n + 31) >> 5;
   const int s = min(lane * k, n), e = min(s + k, n);
   float A = 0.f, B = 1.f;
   for (int i = s; i < e; i++) {
-    const float m = i > 0 ? coef_prev(h, L, i) * ib[(i - 1) * st] : 0.f;
+    const float m = fm[i * st];
     A = fmaf(m, A, rhs[i * st]);
     B *= m;
   }
@@ -127,17 +117,14 @@ __device__ void warp_solve(const HeatDev &h, const LineView &L, float *rhs, cons
   float d = __shfl_up_sync(0xffffffffu, A, 1);
   if (lane == 0) d = 0.f;
   for (int i = s; i < e; i++) {
-    const float m = i > 0 ? coef_prev(h, L, i) * ib[(i - 1) * st] : 0.f;
-    d = fmaf(m, d, rhs[i * st]);
+    d = fmaf(fm[i * st], d, rhs[i * st]);
     rhs[i * st] = d;
   }
-  __syncwarp();
   A = 0.f;
   B = 1.f;
   for (int i = e - 1; i >= s; i--) {
-    const float ibi = ib[i * st];
-    const float f = coef_next(h, L, i) * ibi;
-    A = fmaf(f, A, rhs[i * st] * ibi);
+    const float f = bm[i * st];
+    A = fmaf(f, A, rhs[i * st] * ib[i * st]);
     B *= f;
   }
 #pragma unroll
@@ -152,14 +139,13 @@ __device__ void warp_solve(const HeatDev &h, const LineView &L, float *rhs, cons
   float t = __shfl_down_sync(0xffffffffu, A, 1);
   if (lane == 31) t = 0.f;
   for (int i = e - 1; i >= s; i--) {
-    const float ibi = ib[i * st];
-    t = fmaf(coef_next(h, L, i) * ibi, t, rhs[i * st] * ibi);
+    t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
     rhs[i * st] = t;
   }
   __syncwarp();
 }
 
-// Inverse pivots 1/b'_i of each line's matrix, one thread per line (once per call).
+// Inverse pivots 1/b'_i of each line's matrix, one thread per line (once per call and dt).
 __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
   const int nx = h.nx, ny = h.ny, nz = h.nz;
   const long long nLines = dir == 0 ? (long long)ny * nz : (dir == 1 ? (long long)nx * nz : (long long)nx * ny);
@@ -177,9 +163,8 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
     float bprev = 1.f, ccprev = 0.f;
     for (int i = 0; i < n; i++) {
       const long long v = base + i * st;
-      const bool rowSinked = lineSinked || (h.hs && (i == 0 || i == n - 1));
       float a = 0.f, cc = 0.f;
-      if (!rowSinked) {
+      if (!row_sinked(h, lineSinked, i, n)) {
         const int mi = h.M[v];
         if (i > 0) a = h.hdt * cf(h, mi, h.M[v - st], dir);
         if (i < n - 1) cc = h.hdt * cf(h, mi, h.M[v + st], dir);
@@ -193,15 +178,17 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
   }
 }
 
-// X pass: explicit 1a + solve along x. One warp per x-line; per-warp shared buffers of length nx.
+// X pass: explicit 1a + solve along x. One warp per x-line; per-warp shared lines of length nx
+// (rhs, forward and backward multipliers, inverse pivots).
 __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nx = h.nx, ny = h.ny, nz = h.nz;
   const long long sxy = (long long)nx * ny;
-  float *rhs = (float *)smem + warp * 2 * nx;
-  float *ib = rhs + nx;
-  uint8_t *Ml = (uint8_t *)((float *)smem + 8 * 2 * nx) + warp * nx;
+  float *rhs = (float *)smem + warp * 4 * nx;
+  float *fm = rhs + nx;
+  float *bm = fm + nx;
+  float *ib = bm + nx;
   if (blockIdx.x == 0 && h.nS > 0) record_sensors(h, *h.stepCounter);
   const float *ibx = h.ib;
   for (long long line = blockIdx.x * 8LL + warp; line < (long long)ny * nz; line += gridDim.x * 8LL) {
@@ -211,34 +198,42 @@ __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
     for (int x = lane; x < nx; x += 32) {
       const long long v = base + x;
       const int mi = h.M[v];
-      Ml[x] = (uint8_t)mi;
-      ib[x] = ibx[v];
+      const float ibv = ibx[v];
       const float t = h.T[v];
-      float r = t;
-      if (!lineSinked && !(h.hs && (x == 0 || x == nx - 1))) {
-        float sx = 0.f, syz = 0.f;
-        if (x > 0) sx += cf(h, mi, h.M[v - 1], 0) * (h.T[v - 1] - t);
-        if (x < nx - 1) sx += cf(h, mi, h.M[v + 1], 0) * (h.T[v + 1] - t);
+      float r = t, a = 0.f, cc = 0.f;
+      if (!row_sinked(h, lineSinked, x, nx)) {
+        float syz = 0.f;
+        if (x > 0) a = h.hdt * cf(h, mi, h.M[v - 1], 0);
+        if (x < nx - 1) cc = h.hdt * cf(h, mi, h.M[v + 1], 0);
+        const float sx = (x > 0 ? a * (h.T[v - 1] - t) : 0.f) + (x < nx - 1 ? cc * (h.T[v + 1] - t) : 0.f);
         if (iy > 0) syz += cf(h, mi, h.M[v - nx], 1) * (h.T[v - nx] - t);
         if (iy < ny - 1) syz += cf(h, mi, h.M[v + nx], 1) * (h.T[v + nx] - t);
         if (iz > 0) syz += cf(h, mi, h.M[v - sxy], 2) * (h.T[v - sxy] - t);
         if (iz < nz - 1) syz += cf(h, mi, h.M[v + sxy], 2) * (h.T[v + sxy] - t);
         const float q = h.Q ? h.Q[v] : 0.f;
-        r = t + h.dt * (q + syz) + h.hdt * sx;
+        r = t + h.dt * (q + syz) + sx;
       }
       rhs[x] = r;
+      fm[x] = x > 0 ? a * ibx[v - 1] : 0.f;
+      bm[x] = cc * ibv;
+      ib[x] = ibv;
     }
     __syncwarp();
-    LineView L{Ml, 1, 1, nx, lineSinked, h.hs != 0, 0};
-    warp_solve(h, L, rhs, ib);
+    warp_solve(rhs, fm, bm, ib, nx, 1);
     for (int x = lane; x < nx; x += 32) h.A[base + x] = rhs[x];
     __syncwarp();
   }
 }
 
+template <int TW>
+__host__ __device__ constexpr size_t yz_tile_bytes(int n) {
+  return (size_t)n * (5 * (TW + 1) * 4 + TW);
+}
+
 // Y and Z passes: a block owns TW consecutive x positions and one line per x along `dir`
 // (dir 1: fixed iz; dir 2: fixed iy). Rows of TW floats are read and written coalesced; the
-// tile is solved from shared memory, one warp per line.
+// tile's coefficients are formed in parallel, then each line is solved by one warp from
+// shared memory.
 template <int TW, bool ZPASS>
 __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
@@ -251,7 +246,9 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   float *tn = (float *)smem;
   float *rhs = tn + n * P;
   float *ib = rhs + n * P;
-  uint8_t *Ms = (uint8_t *)(ib + n * P);
+  float *fm = ib + n * P;
+  float *bm = fm + n * P;
+  uint8_t *Ms = (uint8_t *)(bm + n * P);
   __shared__ unsigned int mloc[256];
   const int xTiles = (nx + TW - 1) / TW;
   const int nOther = ZPASS ? ny : nz;
@@ -259,10 +256,13 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   if (ZPASS) {
     for (int k = threadIdx.x; k < h.nM; k += blockDim.x) mloc[k] = 0u;
   }
+  int curM = -1;
+  unsigned int curMax = 0u;
   for (long long tile = blockIdx.x; tile < (long long)xTiles * nOther; tile += gridDim.x) {
     const int x0 = (int)(tile % xTiles) * TW;
     const int other = (int)(tile / xTiles);
     const long long base = ZPASS ? (long long)other * nx : (long long)other * sxy;
+    const bool otherSinked = h.hs && (other == 0 || other == nOther - 1);
     // stage T^n, A, M and pivots
     for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
       const int r = e / TW, cx = e % TW;
@@ -276,29 +276,35 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
       }
     }
     __syncthreads();
-    // explicit half-correction on T^n (2a / 3a)
+    // explicit half-correction on T^n (2a / 3a) and the line multipliers
     for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
       const int r = e / TW, cx = e % TW;
       const int x = x0 + cx;
       if (x >= nx) continue;
-      const int iy = ZPASS ? other : r, iz = ZPASS ? r : other;
-      if (sinked(h, x, iy, iz)) continue;
-      const int mi = Ms[r * TW + cx];
-      const float t = tn[r * P + cx];
-      float s = 0.f;
-      if (r > 0) s += cf(h, mi, Ms[(r - 1) * TW + cx], dir) * (tn[(r - 1) * P + cx] - t);
-      if (r < n - 1) s += cf(h, mi, Ms[(r + 1) * TW + cx], dir) * (tn[(r + 1) * P + cx] - t);
-      rhs[r * P + cx] -= h.hdt * s;
+      const bool lineSinked = otherSinked || (h.hs && (x == 0 || x == nx - 1));
+      float a = 0.f, cc = 0.f;
+      if (!row_sinked(h, lineSinked, r, n)) {
+        const int mi = Ms[r * TW + cx];
+        const float t = tn[r * P + cx];
+        float s = 0.f;
+        if (r > 0) {
+          a = h.hdt * cf(h, mi, Ms[(r - 1) * TW + cx], dir);
+          s += a * (tn[(r - 1) * P + cx] - t);
+        }
+        if (r < n - 1) {
+          cc = h.hdt * cf(h, mi, Ms[(r + 1) * TW + cx], dir);
+          s += cc * (tn[(r + 1) * P + cx] - t);
+        }
+        rhs[r * P + cx] -= s;
+      }
+      fm[r * P + cx] = r > 0 ? a * ib[(r - 1) * P + cx] : 0.f;
+      bm[r * P + cx] = cc * ib[r * P + cx];
     }
     __syncthreads();
     // implicit solves, one warp per line
     for (int cx = threadIdx.x >> 5; cx < TW; cx += blockDim.x >> 5) {
-      const int x = x0 + cx;
-      if (x >= nx) continue;
-      const bool lineSinked = h.hs && (x == 0 || x == nx - 1 || other == 0 || other == nOther - 1);
-      // LineView expects the medium line with stride TW
-      LineView L{Ms + cx, TW, P, n, lineSinked, h.hs != 0, dir};
-      warp_solve(h, L, rhs + cx, ib + cx);
+      if (x0 + cx >= nx) continue;
+      warp_solve(rhs + cx, fm + cx, bm + cx, ib + cx, n, P);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
@@ -309,14 +315,22 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
       const float tnew = rhs[r * P + cx];
       if (ZPASS) {
         const int m = Ms[r * TW + cx];
-        if (h.Omega && h.E[m] != 0.0) {
+        if (h.dOmega && h.E[m] != 0.0) {
           // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602),
           // exponent evaluated in FP64 (logA ~ 154 cancels against E/RT)
           const double tmid = 0.5 * ((double)tnew + (double)tn[r * P + cx]) + h.base + kCelsiusZero;
           const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tmid));
-          h.Omega[v] = (float)((double)h.Omega[v] + h.dtd * rate);
+          h.dOmega[v] += (float)(h.dtd * rate);
         }
-        atomicMax(&mloc[m], enc_max((float)((double)tnew + h.base)));
+        // running per-medium maximum, flushed when this thread's medium changes
+        const unsigned int enc = enc_max((float)((double)tnew + h.base));
+        if (m != curM) {
+          if (curM >= 0) atomicMax(&mloc[curM], curMax);
+          curM = m;
+          curMax = enc;
+        } else if (enc > curMax) {
+          curMax = enc;
+        }
         h.T[v] = tnew;
       } else {
         h.A[v] = tnew;
@@ -325,10 +339,19 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
     __syncthreads();
   }
   if (ZPASS) {
+    if (curM >= 0) atomicMax(&mloc[curM], curMax);
+    __syncthreads();
     for (int k = threadIdx.x; k < h.nM; k += blockDim.x)
       if (mloc[k]) atomicMax(&h.maxEnc[k], mloc[k]);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(h.stepCounter, 1);
   }
+}
+
+// Omega += the damage accumulated over the call (kept apart so the per-step increments are
+// not rounded against Omega's magnitude).
+__global__ void merge_omega_kernel(float *Omega, const float *dOmega, long long L) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < L; k += (long long)gridDim.x * blockDim.x)
+    Omega[k] = (float)((double)Omega[k] + (double)dOmega[k]);
 }
 
 __global__ void final_sensors_kernel(HeatDev h) { record_sensors(h, *h.stepCounter); }
@@ -356,15 +379,19 @@ __global__ void decode_max_kernel(const unsigned int *enc, float *out, int nM) {
 namespace {
 using namespace mcb;
 
+// Widest tile that keeps two blocks per SM (<= 100 KB each), else one block (<= 200 KB).
 int yz_tile_width(int n) {
-  // 13 * (TW + 1) * n bytes of shared memory per tile; stay under ~200 KB
-  if (13LL * 33 * n <= 200000) return 32;
-  if (13LL * 17 * n <= 200000) return 16;
-  if (13LL * 9 * n <= 200000) return 8;
+  if (yz_tile_bytes<32>(n) <= 100000) return 32;
+  if (yz_tile_bytes<16>(n) <= 100000) return 16;
+  if (yz_tile_bytes<8>(n) <= 200000) return 8;
   return 0;
 }
 
-size_t yz_smem(int TW, int n) { return (size_t)n * (3 * (TW + 1) * 4 + TW) + 64; }
+size_t yz_smem(int TW, int n) {
+  return (TW == 32 ? yz_tile_bytes<32>(n) : TW == 16 ? yz_tile_bytes<16>(n) : yz_tile_bytes<8>(n)) + 64;
+}
+
+size_t x_smem(int nx) { return (size_t)8 * 4 * 4 * nx + 64; }
 
 template <int TW>
 mcb_status setup_yz(mcb_ctx *ctx, int ny, int nz) {
@@ -403,7 +430,7 @@ mcb_status check_params(mcb_ctx *ctx, const mcb_heat_params *p) {
     if (!(p->A[m] >= 0) || !(p->E[m] >= 0)) return set_error(ctx, MCB_EINVAL, "A and E must be non-negative");
   if (std::min(yz_tile_width((int)ny), yz_tile_width((int)nz)) == 0)
     return set_error(ctx, MCB_EINVAL, "y or z lines longer than the shared-memory tile limit");
-  if (8LL * 9 * nx + 64 > 200000) return set_error(ctx, MCB_EINVAL, "x lines longer than the shared-memory limit");
+  if (x_smem((int)nx) > 200000) return set_error(ctx, MCB_EINVAL, "x lines longer than the shared-memory limit");
   return MCB_OK;
 }
 
@@ -419,7 +446,8 @@ struct mcb_heat_state {
   double base = 0.0;
   double factoredDt = -1.0;
   int factoredHs = -1;
-  float *T = nullptr, *A = nullptr, *Q = nullptr, *ib = nullptr, *Om = nullptr, *stage = nullptr, *c = nullptr;
+  float *T = nullptr, *A = nullptr, *Q = nullptr, *ib = nullptr, *Om = nullptr, *dOm = nullptr, *stage = nullptr,
+        *c = nullptr;
   uint8_t *M = nullptr;
   double *logA = nullptr, *E = nullptr;
   unsigned int *maxEnc = nullptr;
@@ -445,7 +473,7 @@ void free_state_buffers(mcb_heat_state *s) {
 mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
   const long long L = (long long)p->nx * p->ny * p->nz;
   const int nM = p->nM;
-  const size_t need = 4 * L * 4 /*T A Q stage*/ + 12 * L + (damage ? 4 * L : 0) + L + 12 * (size_t)nM * nM + 16 * (size_t)nM +
+  const size_t need = 4 * L * 4 /*T A Q stage*/ + 12 * L + (damage ? 8 * L : 0) + L + 12 * (size_t)nM * nM + 16 * (size_t)nM +
                       4 * (size_t)nM + 64 + 20 * 256;
   free_state_buffers(s);
   MCB_CUDA(ctx, cudaMalloc(&s->block, need));
@@ -461,6 +489,7 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   s->stage = (float *)take(4 * L);
   s->ib = (float *)take(12 * L);
   s->Om = damage ? (float *)take(4 * L) : nullptr;
+  s->dOm = damage ? (float *)take(4 * L) : nullptr;
   s->M = (uint8_t *)take(L);
   s->c = (float *)take(12 * (size_t)nM * nM);
   s->logA = (double *)take(8 * (size_t)nM);
@@ -505,7 +534,7 @@ HeatDev make_dev(const mcb_heat_state *s, const mcb_heat_params *p) {
   h.nx = s->nx; h.ny = s->ny; h.nz = s->nz; h.nM = s->nM;
   h.T = s->T; h.A = s->A; h.M = s->M; h.c = s->c;
   h.Q = p->lightsOn ? s->Q : nullptr;
-  h.ib = s->ib; h.Omega = s->Om; h.logA = s->logA; h.E = s->E;
+  h.ib = s->ib; h.Omega = s->Om; h.dOmega = s->dOm; h.logA = s->logA; h.E = s->E;
   h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0;
   h.dt = (float)p->dt; h.hdt = (float)(p->dt / 2); h.dtd = p->dt; h.base = s->base;
   h.nS = p->nSensors; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = s->sens; h.stepCounter = s->step;
@@ -544,7 +573,8 @@ mcb_status state_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p,
   }
   MCB_CUDA(ctx, cudaMemsetAsync(s->maxEnc, 0, 4 * (size_t)s->nM, st));
   MCB_CUDA(ctx, cudaMemsetAsync(s->step, 0, 16, st));
-  const size_t smemX = (size_t)8 * nx * 9 + 64;
+  if (s->dOm) MCB_CUDA(ctx, cudaMemsetAsync(s->dOm, 0, 4 * (size_t)L, st));
+  const size_t smemX = x_smem((int)nx);
   MCB_CUDA(ctx, cudaFuncSetAttribute(pass_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemX));
   const int tw = s->tw;
   if (tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
@@ -575,6 +605,7 @@ mcb_status state_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p,
   }
   for (long long k = (nt / chunk) * chunk; k < nt; k++) step(st);
   if (nS) final_sensors_kernel<<<1, 128, 0, st>>>(h);
+  if (s->dOm) merge_omega_kernel<<<grid, 256, 0, st>>>(s->Om, s->dOm, L);
   MCB_CUDA(ctx, cudaGetLastError());
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
   decode_max_kernel<<<1, 256, 0, st>>>(s->maxEnc, s->stage, s->nM);

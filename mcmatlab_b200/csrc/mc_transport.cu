@@ -177,9 +177,8 @@ __global__ void __launch_bounds__(256) transport_kernel(KernelArgs a) {
       if (P.alive) scatter(P, *I);
     }
   }
-  // per-warp reduction of the sub-step count
-  for (int o = 16; o > 0; o >>= 1) steps += __shfl_down_sync(__activemask(), steps, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(a.steps, steps);
+  // lanes leave the loop at different times, so each adds its own count
+  atomicAdd(a.steps, steps);
 }
 
 // (theta, phi) pairs -> unit vectors, as getNormal computes them (MCmatlablib.c:909-918).
