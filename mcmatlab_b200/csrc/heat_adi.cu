@@ -50,6 +50,7 @@ struct HeatDev {
   const double *sIdx, *sW;  // [nS], [nS x 3]
   double *sens;             // [nS x (nt+1)]
   int *stepCounter;
+  int xl;  // x-lines per block in the X pass
 };
 
 __device__ __forceinline__ unsigned int enc_max(float f) {
@@ -145,6 +146,108 @@ __device__ void warp_solve(float *rhs, const float *fm, const float *bm, const f
   __syncwarp();
 }
 
+// Grouped variant for short lines: G lanes (an aligned sub-warp group) share one line, each
+// holding K consecutive elements with fully unrolled chunk loops; 32/G lines are solved by a
+// warp at once. Requires n <= G*K.
+template <int K, int G>
+__device__ __forceinline__ void group_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
+  const int g = threadIdx.x & (G - 1);
+  const int kk = (n + G - 1) / G;  // chunk length (<= K); odd lengths spread the lanes over banks
+  const int s = g * kk;
+  const int e = min(s + kk, n);
+  float A = 0.f, B = 1.f;
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    const int i = s + j;
+    if (i < e) {
+      const float m = fm[i * st];
+      A = fmaf(m, A, rhs[i * st]);
+      B *= m;
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Au = __shfl_up_sync(0xffffffffu, A, off, G);
+    const float Bu = __shfl_up_sync(0xffffffffu, B, off, G);
+    if (g >= off) {
+      A = fmaf(B, Au, A);
+      B *= Bu;
+    }
+  }
+  float d = __shfl_up_sync(0xffffffffu, A, 1, G);
+  if (g == 0) d = 0.f;
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    const int i = s + j;
+    if (i < e) {
+      d = fmaf(fm[i * st], d, rhs[i * st]);
+      rhs[i * st] = d;
+    }
+  }
+  A = 0.f;
+  B = 1.f;
+#pragma unroll
+  for (int j = K - 1; j >= 0; j--) {
+    const int i = s + j;
+    if (i < e) {
+      const float f = bm[i * st];
+      A = fmaf(f, A, rhs[i * st] * ib[i * st]);
+      B *= f;
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Ad = __shfl_down_sync(0xffffffffu, A, off, G);
+    const float Bd = __shfl_down_sync(0xffffffffu, B, off, G);
+    if (g + off < G) {
+      A = fmaf(B, Ad, A);
+      B *= Bd;
+    }
+  }
+  float t = __shfl_down_sync(0xffffffffu, A, 1, G);
+  if (g == G - 1) t = 0.f;
+#pragma unroll
+  for (int j = K - 1; j >= 0; j--) {
+    const int i = s + j;
+    if (i < e) {
+      t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
+      rhs[i * st] = t;
+    }
+  }
+  __syncwarp();
+}
+
+// Lanes per line for the grouped solver (0: use the one-warp-per-line solver).
+__host__ __device__ constexpr int group_lanes(int n) { return n <= 128 ? 8 : (n <= 256 ? 16 : (n <= 512 ? 32 : 0)); }
+
+// Solves `count` lines of one tile; line l starts at base + l*lstride (elements), element
+// stride st. Dispatches on the line length.
+template <int G>
+__device__ __forceinline__ void solve_lines_g(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
+                                              int lstride, int count) {
+  constexpr int LPW = 32 / G;  // lines per warp at once
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int sub = (threadIdx.x & 31) / G;
+  for (int l0 = warp * LPW; l0 < count; l0 += nw * LPW) {
+    const int l = l0 + sub;
+    // groups without a line run the same shuffles on an empty line so the warp stays converged
+    if (l < count) group_solve<16, G>(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
+    else group_solve<16, G>(rhs, fm, bm, ib, 0, st);
+  }
+}
+
+__device__ __forceinline__ void solve_lines(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
+                                            int lstride, int count) {
+  const int G = group_lanes(n);
+  if (G == 8) solve_lines_g<8>(rhs, fm, bm, ib, n, st, lstride, count);
+  else if (G == 16) solve_lines_g<16>(rhs, fm, bm, ib, n, st, lstride, count);
+  else if (G == 32) solve_lines_g<32>(rhs, fm, bm, ib, n, st, lstride, count);
+  else {
+    for (int l = threadIdx.x >> 5; l < count; l += blockDim.x >> 5)
+      warp_solve(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
+  }
+}
+
 // Inverse pivots 1/b'_i of each line's matrix, one thread per line (once per call and dt).
 __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
   const int nx = h.nx, ny = h.ny, nz = h.nz;
@@ -178,50 +281,81 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
   }
 }
 
-// X pass: explicit 1a + solve along x. One warp per x-line; per-warp shared lines of length nx
-// (rhs, forward and backward multipliers, inverse pivots).
+// X pass: explicit 1a + solve along x. A block owns h.xl consecutive x-lines (consecutive y at
+// one z); each line's rhs, multipliers and pivots are formed in shared memory, then the lines
+// are solved together.
+
 __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nx = h.nx, ny = h.ny, nz = h.nz;
-  const long long sxy = (long long)nx * ny;
-  float *rhs = (float *)smem + warp * 4 * nx;
-  float *fm = rhs + nx;
-  float *bm = fm + nx;
-  float *ib = bm + nx;
+  const int sxy = nx * ny;
+  const int P = nx + 1;  // line pitch
+  const int XL = h.xl;
+  float *rhs = (float *)smem;
+  float *fm = rhs + XL * P;
+  float *bm = fm + XL * P;
+  float *ib = bm + XL * P;
   if (blockIdx.x == 0 && h.nS > 0) record_sensors(h, *h.stepCounter);
   const float *ibx = h.ib;
-  for (long long line = blockIdx.x * 8LL + warp; line < (long long)ny * nz; line += gridDim.x * 8LL) {
-    const int iy = (int)(line % ny), iz = (int)(line / ny);
-    const long long base = (long long)iy * nx + iz * sxy;
-    const bool lineSinked = h.hs && (iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1);
-    for (int x = lane; x < nx; x += 32) {
-      const long long v = base + x;
-      const int mi = h.M[v];
-      const float ibv = ibx[v];
-      const float t = h.T[v];
-      float r = t, a = 0.f, cc = 0.f;
-      if (!row_sinked(h, lineSinked, x, nx)) {
-        float syz = 0.f;
-        if (x > 0) a = h.hdt * cf(h, mi, h.M[v - 1], 0);
-        if (x < nx - 1) cc = h.hdt * cf(h, mi, h.M[v + 1], 0);
-        const float sx = (x > 0 ? a * (h.T[v - 1] - t) : 0.f) + (x < nx - 1 ? cc * (h.T[v + 1] - t) : 0.f);
-        if (iy > 0) syz += cf(h, mi, h.M[v - nx], 1) * (h.T[v - nx] - t);
-        if (iy < ny - 1) syz += cf(h, mi, h.M[v + nx], 1) * (h.T[v + nx] - t);
-        if (iz > 0) syz += cf(h, mi, h.M[v - sxy], 2) * (h.T[v - sxy] - t);
-        if (iz < nz - 1) syz += cf(h, mi, h.M[v + sxy], 2) * (h.T[v + sxy] - t);
-        const float q = h.Q ? h.Q[v] : 0.f;
-        r = t + h.dt * (q + syz) + sx;
+  const int yTiles = (ny + XL - 1) / XL;
+  for (int tile = blockIdx.x; tile < yTiles * nz; tile += gridDim.x) {
+    const int y0 = (tile % yTiles) * XL, iz = tile / yTiles;
+    const int cnt = min(XL, ny - y0);
+    const int total = cnt * nx;
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < total; e0 += blockDim.x * U) {
+      float vr[U], vf[U], vb[U], vi[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int e = e0 + u * blockDim.x;
+        vr[u] = vf[u] = vb[u] = vi[u] = 0.f;
+        if (e < total) {
+          const int l = e / nx, x = e - l * nx;
+          const int iy = y0 + l;
+          const int v = x + iy * nx + iz * sxy;
+          const bool lineSinked = h.hs && (iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1);
+          const int mi = h.M[v];
+          const float ibv = ibx[v];
+          const float t = h.T[v];
+          float r = t, a = 0.f, cc = 0.f;
+          if (!row_sinked(h, lineSinked, x, nx)) {
+            float syz = 0.f;
+            if (x > 0) a = h.hdt * cf(h, mi, h.M[v - 1], 0);
+            if (x < nx - 1) cc = h.hdt * cf(h, mi, h.M[v + 1], 0);
+            const float sx = (x > 0 ? a * (h.T[v - 1] - t) : 0.f) + (x < nx - 1 ? cc * (h.T[v + 1] - t) : 0.f);
+            if (iy > 0) syz += cf(h, mi, h.M[v - nx], 1) * (h.T[v - nx] - t);
+            if (iy < ny - 1) syz += cf(h, mi, h.M[v + nx], 1) * (h.T[v + nx] - t);
+            if (iz > 0) syz += cf(h, mi, h.M[v - sxy], 2) * (h.T[v - sxy] - t);
+            if (iz < nz - 1) syz += cf(h, mi, h.M[v + sxy], 2) * (h.T[v + sxy] - t);
+            const float q = h.Q ? h.Q[v] : 0.f;
+            r = t + h.dt * (q + syz) + sx;
+          }
+          vr[u] = r;
+          vf[u] = x > 0 ? a * ibx[v - 1] : 0.f;
+          vb[u] = cc * ibv;
+          vi[u] = ibv;
+        }
       }
-      rhs[x] = r;
-      fm[x] = x > 0 ? a * ibx[v - 1] : 0.f;
-      bm[x] = cc * ibv;
-      ib[x] = ibv;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int e = e0 + u * blockDim.x;
+        if (e < total) {
+          const int l = e / nx, x = e - l * nx;
+          rhs[l * P + x] = vr[u];
+          fm[l * P + x] = vf[u];
+          bm[l * P + x] = vb[u];
+          ib[l * P + x] = vi[u];
+        }
+      }
     }
-    __syncwarp();
-    warp_solve(rhs, fm, bm, ib, nx, 1);
-    for (int x = lane; x < nx; x += 32) h.A[base + x] = rhs[x];
-    __syncwarp();
+    __syncthreads();
+    solve_lines(rhs, fm, bm, ib, nx, 1, P, cnt);
+    __syncthreads();
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / nx, x = e - l * nx;
+      h.A[x + (y0 + l) * nx + iz * sxy] = rhs[l * P + x];
+    }
+    __syncthreads();
   }
 }
 
@@ -231,17 +365,17 @@ __host__ __device__ constexpr size_t yz_tile_bytes(int n) {
 }
 
 // Y and Z passes: a block owns TW consecutive x positions and one line per x along `dir`
-// (dir 1: fixed iz; dir 2: fixed iy). Rows of TW floats are read and written coalesced; the
-// tile's coefficients are formed in parallel, then each line is solved by one warp from
-// shared memory.
+// (dir 1: fixed iz; dir 2: fixed iy). Rows of TW values are read and written coalesced (loads
+// batched per thread for memory-level parallelism); coefficients are formed in parallel, then
+// the TW lines are solved together from shared memory.
 template <int TW, bool ZPASS>
 __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
   constexpr int P = TW + 1;  // padded pitch
   const int nx = h.nx, ny = h.ny, nz = h.nz;
-  const long long sxy = (long long)nx * ny;
+  const int sxy = nx * ny;
   const int n = ZPASS ? nz : ny;
-  const long long st = ZPASS ? sxy : nx;
+  const int st = ZPASS ? sxy : nx;
   const int dir = ZPASS ? 2 : 1;
   float *tn = (float *)smem;
   float *rhs = tn + n * P;
@@ -252,88 +386,100 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   __shared__ unsigned int mloc[256];
   const int xTiles = (nx + TW - 1) / TW;
   const int nOther = ZPASS ? ny : nz;
-  const float *ibd = h.ib + (long long)dir * sxy * nz;
+  const float *ibd = h.ib + (size_t)dir * sxy * nz;
   if (ZPASS) {
     for (int k = threadIdx.x; k < h.nM; k += blockDim.x) mloc[k] = 0u;
   }
   int curM = -1;
   unsigned int curMax = 0u;
-  for (long long tile = blockIdx.x; tile < (long long)xTiles * nOther; tile += gridDim.x) {
-    const int x0 = (int)(tile % xTiles) * TW;
-    const int other = (int)(tile / xTiles);
-    const long long base = ZPASS ? (long long)other * nx : (long long)other * sxy;
+  constexpr int RPI = 256 / TW;  // rows covered by one pass of the block
+  constexpr int U = 4;
+  const int cx = threadIdx.x % TW, r0 = threadIdx.x / TW;
+  for (int tile = blockIdx.x; tile < xTiles * nOther; tile += gridDim.x) {
+    const int x0 = (tile % xTiles) * TW;
+    const int other = tile / xTiles;
+    const int base = ZPASS ? other * nx : other * sxy;
     const bool otherSinked = h.hs && (other == 0 || other == nOther - 1);
+    const int x = x0 + cx;
     // stage T^n, A, M and pivots
-    for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
-      const int r = e / TW, cx = e % TW;
-      const int x = x0 + cx;
-      if (x < nx) {
-        const long long v = base + x + r * st;
-        tn[r * P + cx] = h.T[v];
-        rhs[r * P + cx] = h.A[v];
-        ib[r * P + cx] = ibd[v];
-        Ms[r * TW + cx] = h.M[v];
+    for (int rb = r0; rb < n; rb += RPI * U) {
+      float vT[U], vA[U], vI[U];
+      uint8_t vM[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int r = rb + u * RPI;
+        if (r < n && x < nx) {
+          const int v = base + x + r * st;
+          vT[u] = h.T[v];
+          vA[u] = h.A[v];
+          vI[u] = ibd[v];
+          vM[u] = h.M[v];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int r = rb + u * RPI;
+        if (r < n && x < nx) {
+          tn[r * P + cx] = vT[u];
+          rhs[r * P + cx] = vA[u];
+          ib[r * P + cx] = vI[u];
+          Ms[r * TW + cx] = vM[u];
+        }
       }
     }
     __syncthreads();
     // explicit half-correction on T^n (2a / 3a) and the line multipliers
-    for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
-      const int r = e / TW, cx = e % TW;
-      const int x = x0 + cx;
-      if (x >= nx) continue;
+    if (x < nx) {
       const bool lineSinked = otherSinked || (h.hs && (x == 0 || x == nx - 1));
-      float a = 0.f, cc = 0.f;
-      if (!row_sinked(h, lineSinked, r, n)) {
-        const int mi = Ms[r * TW + cx];
-        const float t = tn[r * P + cx];
-        float s = 0.f;
-        if (r > 0) {
-          a = h.hdt * cf(h, mi, Ms[(r - 1) * TW + cx], dir);
-          s += a * (tn[(r - 1) * P + cx] - t);
+      for (int r = r0; r < n; r += RPI) {
+        float a = 0.f, cc = 0.f;
+        if (!row_sinked(h, lineSinked, r, n)) {
+          const int mi = Ms[r * TW + cx];
+          const float t = tn[r * P + cx];
+          float sm = 0.f;
+          if (r > 0) {
+            a = h.hdt * cf(h, mi, Ms[(r - 1) * TW + cx], dir);
+            sm += a * (tn[(r - 1) * P + cx] - t);
+          }
+          if (r < n - 1) {
+            cc = h.hdt * cf(h, mi, Ms[(r + 1) * TW + cx], dir);
+            sm += cc * (tn[(r + 1) * P + cx] - t);
+          }
+          rhs[r * P + cx] -= sm;
         }
-        if (r < n - 1) {
-          cc = h.hdt * cf(h, mi, Ms[(r + 1) * TW + cx], dir);
-          s += cc * (tn[(r + 1) * P + cx] - t);
-        }
-        rhs[r * P + cx] -= s;
+        fm[r * P + cx] = r > 0 ? a * ib[(r - 1) * P + cx] : 0.f;
+        bm[r * P + cx] = cc * ib[r * P + cx];
       }
-      fm[r * P + cx] = r > 0 ? a * ib[(r - 1) * P + cx] : 0.f;
-      bm[r * P + cx] = cc * ib[r * P + cx];
     }
     __syncthreads();
-    // implicit solves, one warp per line
-    for (int cx = threadIdx.x >> 5; cx < TW; cx += blockDim.x >> 5) {
-      if (x0 + cx >= nx) continue;
-      warp_solve(rhs + cx, fm + cx, bm + cx, ib + cx, n, P);
-    }
+    solve_lines(rhs, fm, bm, ib, n, P, 1, min(TW, nx - x0));
     __syncthreads();
-    for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
-      const int r = e / TW, cx = e % TW;
-      const int x = x0 + cx;
-      if (x >= nx) continue;
-      const long long v = base + x + r * st;
-      const float tnew = rhs[r * P + cx];
-      if (ZPASS) {
-        const int m = Ms[r * TW + cx];
-        if (h.dOmega && h.E[m] != 0.0) {
-          // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602),
-          // exponent evaluated in FP64 (logA ~ 154 cancels against E/RT)
-          const double tmid = 0.5 * ((double)tnew + (double)tn[r * P + cx]) + h.base + kCelsiusZero;
-          const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tmid));
-          h.dOmega[v] += (float)(h.dtd * rate);
+    if (x < nx) {
+      for (int r = r0; r < n; r += RPI) {
+        const int v = base + x + r * st;
+        const float tnew = rhs[r * P + cx];
+        if (ZPASS) {
+          const int m = Ms[r * TW + cx];
+          if (h.dOmega && h.E[m] != 0.0) {
+            // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602),
+            // exponent evaluated in FP64 (logA ~ 154 cancels against E/RT)
+            const double tmid = 0.5 * ((double)tnew + (double)tn[r * P + cx]) + h.base + kCelsiusZero;
+            const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tmid));
+            h.dOmega[v] += (float)(h.dtd * rate);
+          }
+          // running per-medium maximum, flushed when this thread's medium changes
+          const unsigned int enc = enc_max((float)((double)tnew + h.base));
+          if (m != curM) {
+            if (curM >= 0) atomicMax(&mloc[curM], curMax);
+            curM = m;
+            curMax = enc;
+          } else if (enc > curMax) {
+            curMax = enc;
+          }
+          h.T[v] = tnew;
+        } else {
+          h.A[v] = tnew;
         }
-        // running per-medium maximum, flushed when this thread's medium changes
-        const unsigned int enc = enc_max((float)((double)tnew + h.base));
-        if (m != curM) {
-          if (curM >= 0) atomicMax(&mloc[curM], curMax);
-          curM = m;
-          curMax = enc;
-        } else if (enc > curMax) {
-          curMax = enc;
-        }
-        h.T[v] = tnew;
-      } else {
-        h.A[v] = tnew;
       }
     }
     __syncthreads();
@@ -391,7 +537,16 @@ size_t yz_smem(int TW, int n) {
   return (TW == 32 ? yz_tile_bytes<32>(n) : TW == 16 ? yz_tile_bytes<16>(n) : yz_tile_bytes<8>(n)) + 64;
 }
 
-size_t x_smem(int nx) { return (size_t)8 * 4 * 4 * nx + 64; }
+size_t x_smem_lines(int nx, int xl) { return (size_t)xl * 4 * 4 * (nx + 1) + 64; }
+
+// x-lines per X-pass block: the most that keeps the block's shared memory within 100 KB
+int x_lines(int nx) {
+  for (int xl = 32; xl >= 2; xl >>= 1)
+    if (x_smem_lines(nx, xl) <= 100000) return xl;
+  return x_smem_lines(nx, 1) <= 200000 ? 1 : 0;
+}
+
+size_t x_smem(int nx) { return x_smem_lines(nx, x_lines(nx)); }
 
 template <int TW>
 mcb_status setup_yz(mcb_ctx *ctx, int ny, int nz) {
@@ -430,7 +585,7 @@ mcb_status check_params(mcb_ctx *ctx, const mcb_heat_params *p) {
     if (!(p->A[m] >= 0) || !(p->E[m] >= 0)) return set_error(ctx, MCB_EINVAL, "A and E must be non-negative");
   if (std::min(yz_tile_width((int)ny), yz_tile_width((int)nz)) == 0)
     return set_error(ctx, MCB_EINVAL, "y or z lines longer than the shared-memory tile limit");
-  if (x_smem((int)nx) > 200000) return set_error(ctx, MCB_EINVAL, "x lines longer than the shared-memory limit");
+  if (x_lines((int)nx) == 0) return set_error(ctx, MCB_EINVAL, "x lines longer than the shared-memory limit");
   return MCB_OK;
 }
 
@@ -538,6 +693,7 @@ HeatDev make_dev(const mcb_heat_state *s, const mcb_heat_params *p) {
   h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0;
   h.dt = (float)p->dt; h.hdt = (float)(p->dt / 2); h.dtd = p->dt; h.base = s->base;
   h.nS = p->nSensors; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = s->sens; h.stepCounter = s->step;
+  h.xl = x_lines(s->nx);
   return h;
 }
 
@@ -580,8 +736,8 @@ mcb_status state_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p,
   if (tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
   else if (tw == 16) MCB_TRY(setup_yz<16>(ctx, (int)ny, (int)nz));
   else MCB_TRY(setup_yz<8>(ctx, (int)ny, (int)nz));
-  const long long linesX = ny * nz;
-  const int gridX = (int)std::min<long long>((linesX + 7) / 8, (long long)ctx->num_sms * 64);
+  const long long tilesX = ((ny + h.xl - 1) / h.xl) * nz;
+  const int gridX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * 64);
   const long long tiles = ((nx + tw - 1) / tw) * std::max(ny, nz);
   const int gridYZ = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 64);
   auto step = [&](cudaStream_t q) {

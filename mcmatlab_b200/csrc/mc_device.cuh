@@ -32,6 +32,7 @@ struct Inst {
   int ffr;  // farFieldRes
   const uint8_t *M0;    // 0-based medium per voxel
   const float4 *nrm;    // unit interface normal per voxel, or nullptr (matched interfaces)
+  int nM;
   const float4 *med;    // per medium: mua, mus, g, RI
   const int *cdfidx;    // per medium
   const float *CDFs;    // [201 x nCDF]

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -41,6 +42,9 @@ struct KernelArgs {
   const volatile int *cancel;        // host-mapped cancel flag
   int *status;                       // bit 0: cancelled, bit 1: a launch failed 1e6 times
   unsigned long long *steps;
+  // Refill threshold: a warp re-launches free lanes only when at least this many are free (or
+  // none is alive), so the divergent launch code runs once for a group of lanes.
+  int refillMin;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -89,92 +93,126 @@ __device__ __forceinline__ unsigned long long fetch_packet(const KernelArgs &a) 
   return g;
 }
 
-__global__ void __launch_bounds__(256) transport_kernel(KernelArgs a) {
+
+__global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
+  // single-instance runs read the instance and its medium table from shared memory
+  __shared__ Inst sInst;
+  __shared__ float4 sMed[256];
+  __shared__ int sCdf[256];
+  const bool single = a.nInst == 1;
+  if (single) {
+    const Inst *g0 = a.insts;
+    if (threadIdx.x == 0) sInst = *g0;
+    for (int k = threadIdx.x; k < g0->nM; k += blockDim.x) {
+      sMed[k] = g0->med[k];
+      sCdf[k] = g0->cdfidx[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sInst.med = sMed;
+      sInst.cdfidx = sCdf;
+    }
+    __syncthreads();
+  }
   Photon P;
   P.alive = false;
-  const Inst *I = nullptr;
+  const Inst *I = single ? &sInst : a.insts;
   bool replay = false;
   bool started = false;
+  bool retired = false;
   float wfinal = 0.f;
   double acc = 0.0;
   int accj = -1;
   unsigned long long steps = 0;
   unsigned long long pid = 0;
   for (;;) {
-    if (!P.alive) {
-      if (started) {
-        if (accj >= 0) {
-          atomic_add_f64(&I->NFR[accj], acc);
-          accj = -1;
-          acc = 0.0;
-        }
-        if (I->eol && !replay && I->NFR && criteria_met(P, *I)) {
-          // replay the same packet, depositing w_final * absorb (MCmatlab.c:262-264)
-          replay = true;
-          wfinal = P.weight;
-          P.pidlo = (uint32_t)pid;
-          P.pidhi = (uint32_t)(pid >> 32);
-          P.draw = 0;
-          launch_packet(P, *I);
-          voxel_props(P, *I);
-          continue;
-        }
+    // 1. a finished packet: flush its deposit run, then either start its end-of-life replay
+    //    (MCmatlab.c:262-264) or mark the lane free
+    if (!P.alive && started) {
+      if (accj >= 0) {
+        atomic_add_f64(&I->NFR[accj], acc);
+        accj = -1;
+        acc = 0.0;
+      }
+      if (I->eol && !replay && I->NFR && criteria_met(P, *I)) {
+        replay = true;
+        wfinal = P.weight;
+        P.pidlo = (uint32_t)pid;
+        P.pidhi = (uint32_t)(pid >> 32);
+        P.draw = 0;
+        launch_packet(P, *I);
+        voxel_props(P, *I);
+      } else {
         replay = false;
         started = false;
       }
-      const unsigned long long g = fetch_packet(a);
-      if (g == ~0ull) break;
-      const int ii = find_instance(a, g);
-      I = a.insts + ii;
-      pid = g - __ldg(a.instFirst + ii);
-      P.pidlo = (uint32_t)pid;
-      P.pidhi = (uint32_t)(pid >> 32);
-      P.draw = 0;
-      if (!launch_packet(P, *I)) {
-        atomicAdd(&I->ctr[3], 1ull);
-        atomicOr(a.status, 2);
-        continue;
-      }
-      voxel_props(P, *I);
-      atomicAdd(&I->ctr[0], 1ull);
-      started = true;
-      continue;
     }
-    if (P.stepLeft > 0) {
-      const float s = propagate(P, *I);
-      steps++;
-      const float absorb = -P.weight * expm1f(-P.mua * s);
-      P.weight -= absorb;
-      if (P.inside && I->NFR) {
-        double c = 0.0;
-        bool dep = false;
-        if (replay) {
-          c = (double)wfinal * (double)absorb;
-          dep = true;
-        } else if (!I->eol && criteria_met(P, *I)) {
-          c = (double)absorb;
-          dep = true;
-        }
-        if (dep) {
-          if (P.j == accj) {
-            acc += c;
+    // 2. refill free lanes in groups
+    const unsigned freeLanes = __ballot_sync(0xffffffffu, !P.alive && !retired);
+    const unsigned liveLanes = __ballot_sync(0xffffffffu, P.alive);
+    if (freeLanes && (__popc(freeLanes) >= a.refillMin || liveLanes == 0)) {
+      if (!P.alive && !retired) {
+        const unsigned long long g = fetch_packet(a);
+        if (g == ~0ull) {
+          retired = true;
+        } else {
+          const int ii = single ? 0 : find_instance(a, g);
+          if (!single) I = a.insts + ii;
+          pid = g - (single ? 0ull : __ldg(a.instFirst + ii));
+          P.pidlo = (uint32_t)pid;
+          P.pidhi = (uint32_t)(pid >> 32);
+          P.draw = 0;
+          if (launch_packet(P, *I)) {
+            voxel_props(P, *I);
+            atomicAdd(&I->ctr[0], 1ull);
+            started = true;
           } else {
-            if (accj >= 0) atomic_add_f64(&I->NFR[accj], acc);
-            accj = P.j;
-            acc = c;
+            atomicAdd(&I->ctr[3], 1ull);
+            atomicOr(a.status, 2);
           }
         }
       }
-      if (!P.sameVoxel) {
-        check_escape(P, *I, !replay);
-        if (P.alive) voxel_props(P, *I);
+    }
+    if (__all_sync(0xffffffffu, retired && !P.alive)) break;
+    // 3. one propagation sub-step, then the scattering event if the free path is used up
+    if (P.alive) {
+      if (P.stepLeft > 0) {
+        const float s = propagate(P, *I);
+        steps++;
+        const float absorb = -P.weight * expm1f(-P.mua * s);
+        P.weight -= absorb;
+        if (P.inside && I->NFR) {
+          double c = 0.0;
+          bool dep = false;
+          if (replay) {
+            c = (double)wfinal * (double)absorb;
+            dep = true;
+          } else if (!I->eol && criteria_met(P, *I)) {
+            c = (double)absorb;
+            dep = true;
+          }
+          if (dep) {
+            if (P.j == accj) {
+              acc += c;
+            } else {
+              if (accj >= 0) atomic_add_f64(&I->NFR[accj], acc);
+              accj = P.j;
+              acc = c;
+            }
+          }
+        }
+        if (!P.sameVoxel) {
+          check_escape(P, *I, !replay);
+          if (P.alive) voxel_props(P, *I);
+        }
       }
-    } else {
-      if (P.weight < kThreshold) {
-        if (rnd(P, *I) <= kChance) P.weight /= kChance;
-        else P.alive = false;
+      if (P.alive && !(P.stepLeft > 0)) {
+        if (P.weight < kThreshold) {
+          if (rnd(P, *I) <= kChance) P.weight /= kChance;
+          else P.alive = false;
+        }
+        if (P.alive) scatter(P, *I);
       }
-      if (P.alive) scatter(P, *I);
     }
   }
   // lanes leave the loop at different times, so each adds its own count
@@ -606,6 +644,7 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     I.ffr = m->farFieldRes;
     I.M0 = pl.M0;
     I.nrm = pl.nrm;
+    I.nM = nM;
     I.med = pl.med + (size_t)iL * nM;
     I.cdfidx = pl.cdfidx + (size_t)iL * nM;
     I.CDFs = pl.CDFs;
@@ -702,6 +741,8 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
   a.collectTarget = collectTarget;
   a.cancel = ctx->cancel_dev;
   a.deadlineNs = 0;
+  a.refillMin = 8;
+  if (const char *e = std::getenv("MCB_REFILL_MIN")) a.refillMin = std::max(1, std::min(32, std::atoi(e)));
   int blocksPerSm = 0;
   MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, transport_kernel, 256, 0));
   if (blocksPerSm < 1) blocksPerSm = 1;
