@@ -190,11 +190,11 @@ __device__ __forceinline__ void direction_changed(Photon &P, const Inst &I) {
 __device__ __forceinline__ void voxel_props(Photon &P, const Inst &I) {
   P.j = voxel_index(I, P.i);
   const int m = __ldg(I.M0 + P.j);
-  const float4 mp = __ldg(I.med + m);
+  const float4 mp = I.med[m];
   P.mua = mp.x;
   P.mus = mp.y;
   P.g = mp.z;
-  P.cdf = __ldg(I.cdfidx + m);
+  P.cdf = I.cdfidx[m];
 }
 
 __device__ __forceinline__ float launch_time(const Photon &P, const Inst &I, const float *t) {
@@ -227,7 +227,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
       P.u[1] = st * sp;
       P.u[2] = ct;
       P.j = voxel_index(I, P.i);
-      P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+      P.RI = I.med[__ldg(I.M0 + P.j)].w;
       P.time = 0;
     } else {
       switch (I.beamType) {
@@ -237,7 +237,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.i[2] = 0;
           for (int k = 0; k < 3; k++) P.u[k] = I.u[k];
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = launch_time(P, I, I.focus);
           break;
         case 1: {
@@ -254,7 +254,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.u[1] = st * sp;
           P.u[2] = ct;
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = 0;
           break;
         }
@@ -265,7 +265,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.i[2] = 0;
           for (int k = 0; k < 3; k++) P.u[k] = I.u[k];
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = P.RI / kC *
                    ((P.i[0] - I.n[0] / 2.0f) * I.d[0] * I.u[0] + (P.i[1] - I.n[1] / 2.0f) * I.d[1] * I.u[1] + P.i[2] * I.d[2] * I.u[2]);
           break;
@@ -281,7 +281,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.i[1] = (tgt[1] - tgt[2] * P.u[1] / P.u[2]) / I.d[1] + I.n[1] / 2.0f;
           P.i[2] = 0;
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = launch_time(P, I, tgt);
           break;
         }
@@ -311,7 +311,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.i[1] = (tgt[1] - tgt[2] * P.u[1] / P.u[2]) / I.d[1] + I.n[1] / 2.0f;
           P.i[2] = 0;
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = launch_time(P, I, tgt);
           break;
         }
@@ -367,7 +367,7 @@ __device__ bool launch_packet(Photon &P, const Inst &I) {
           P.i[1] = (tgt[1] - tgt[2] * P.u[1] / P.u[2]) / I.d[1] + I.n[1] / 2.0f;
           P.i[2] = 0;
           P.j = voxel_index(I, P.i);
-          P.RI = __ldg(I.med + __ldg(I.M0 + P.j)).w;
+          P.RI = I.med[__ldg(I.M0 + P.j)].w;
           P.time = launch_time(P, I, tgt);
           break;
         }
@@ -397,7 +397,7 @@ __device__ __forceinline__ void interface_normal(const Photon &P, const Inst &I,
   for (int k = 0; k < 3; k++) {
     i0[k] = clamp_coord(P.i[k], I.n[k]) - 1;
   }
-  const float ri = __ldg(I.med + __ldg(I.M0 + jn)).w;
+  const float ri = I.med[__ldg(I.M0 + jn)].w;
   float sx = 0.f, sy = 0.f, sz = 0.f;
 #pragma unroll
   for (int c = 0; c < 8; c++) {
@@ -407,7 +407,7 @@ __device__ __forceinline__ void interface_normal(const Photon &P, const Inst &I,
                     (cz ? i0[2] < I.n[2] - 1 : jz >= 0);
     if (!ok) continue;
     const int jc = (jz * I.n[1] + jy) * I.n[0] + jx;
-    if (__ldg(I.med + __ldg(I.M0 + jc)).w != ri) continue;
+    if (I.med[__ldg(I.M0 + jc)].w != ri) continue;
     const float4 nn = __ldg(I.nrm + jc);
     sx += nn.x;
     sy += nn.y;
@@ -442,7 +442,7 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
   if (!P.sameVoxel) {
     const int jn = voxel_index(I, P.i);
     const int mn = __ldg(I.M0 + jn);
-    const float rin = __ldg(I.med + mn).w;
+    const float rin = I.med[mn].w;
     const float mu = P.RI / rin;
     if (mu != 1.f) {
       float nv[3];
@@ -475,7 +475,7 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
       }
     } else {
       const int mo = __ldg(I.M0 + P.j);
-      if (mn != mo && __ldg(I.med + mo).w == P.RI && (uint32_t)mn >= I.minIdx && (uint32_t)mn <= I.maxIdx) P.itr++;
+      if (mn != mo && I.med[mo].w == P.RI && (uint32_t)mn >= I.minIdx && (uint32_t)mn <= I.maxIdx) P.itr++;
     }
   }
   return s;
