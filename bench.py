@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 from mcmatlab_b200 import configs, mexargs, prep  # noqa: E402
 
 METRIC = "photon packets/s, heat voxel-updates/s on 1 B200; batched+adjoint vs plain"
+HEAT_STEP_DRAM_BYTES = 39.4e6
 N_GRID = 100
 MC_PACKETS = 1_000_000
 
@@ -206,7 +207,10 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(L * 8 + 4 * len(th["VHC"])),
                 "timing": "wall clock around mcb_heat_forward (host buffers)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": src, "traffic": None,
+                     "peak_source": src,
+                     # DRAM bytes of one DG-ADI step (X + Y + Z pass) from the cold-cache ncu capture
+                     # (profiles/heat_dgadi_c1_100cube.md); in the timed loop the grid is L2-resident
+                     "traffic": HEAT_STEP_DRAM_BYTES, "traffic_note": "ncu cold-cache capture, bytes per DG-ADI step",
                      "algorithmic_bytes_per_voxel_update": bytes_per_update,
                      "kernel": "DG-ADI step (pass_x + pass_yz<y> + pass_yz<z>)"},
         "gpu_launches": launches,
