@@ -81,6 +81,12 @@ bool mxIsNaN(double x);
 bool mxIsInf(double x);
 bool mxIsFinite(double x);
 
+/* memory and exit hooks */
+void *mxMalloc(size_t n);
+void *mxCalloc(size_t n, size_t size);
+void  mxFree(void *ptr);
+int   mexAtExit(void (*fn)(void));
+
 /* MEX services */
 int  mexPrintf(const char *fmt, ...);
 int  mexEvalString(const char *cmd);

@@ -216,13 +216,15 @@ MXS_EXPORT void mxSetField(mxArray *pa, mwIndex i, const char *fieldname, mxArra
   (void)i;
   set_named(pa, fieldname, value);
 }
+/* As in MATLAB, a property that does not exist yields NULL. */
 MXS_EXPORT mxArray *mxGetProperty(const mxArray *pa, mwIndex i, const char *propname) {
   (void)i;
-  return get_named(pa, propname, "property");
+  if (!pa || !pa->is_bag) return NULL;
+  int k = find_field(pa, propname);
+  return k < 0 ? NULL : pa->values[k];
 }
 MXS_EXPORT mxArray *mxGetPropertyShared(const mxArray *pa, mwIndex i, const char *propname) {
-  (void)i;
-  return get_named(pa, propname, "property");
+  return mxGetProperty(pa, i, propname);
 }
 MXS_EXPORT void mxSetProperty(mxArray *pa, mwIndex i, const char *propname, const mxArray *value) {
   (void)i;
@@ -257,6 +259,14 @@ MXS_EXPORT void mexErrMsgIdAndTxt(const char *id, const char *fmt, ...) {
 MXS_EXPORT void mexErrMsgTxt(const char *msg) { fail("MEX", msg); }
 
 MXS_EXPORT bool utIsInterruptPending(void) { return false; }
+
+MXS_EXPORT void *mxMalloc(size_t n) { return malloc(n ? n : 1); }
+MXS_EXPORT void *mxCalloc(size_t n, size_t size) { return calloc(n ? n : 1, size ? size : 1); }
+MXS_EXPORT void mxFree(void *ptr) { free(ptr); }
+MXS_EXPORT int mexAtExit(void (*fn)(void)) {
+  (void)fn;
+  return 0;
+}
 
 /* ---- harness helpers (bag introspection, guarded calls) ---- */
 MXS_EXPORT int mxshim_is_bag(const mxArray *pa) { return pa ? pa->is_bag : 0; }

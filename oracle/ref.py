@@ -135,13 +135,14 @@ def shim():
 
 
 class RefMC:
-    """The reference MC MEX (MCmatlab.c) on the host cores."""
+    """The reference MC MEX (MCmatlab.c) on the host cores. With libname="libmex_mc_cuda.so"
+    the same harness drives this library's MEX gateway (mcmatlab_b200/mex/MCmatlab_CUDA.c)."""
     OUTPUTS = ("NFR", "farField", "NI_xpos", "NI_xneg", "NI_ypos", "NI_yneg", "NI_zpos", "NI_zneg",
                "nPhotons", "nPhotonsCollected", "nThreads", "simulationTime", "examplePaths")
 
-    def __init__(self):
+    def __init__(self, libname="libref_mc.so"):
         self.sh = shim()
-        self.lib = C.CDLL(os.path.join(REF_DIR, "libref_mc.so"))
+        self.lib = C.CDLL(os.path.join(REF_DIR, libname))
         self.fn = self.lib.mexFunction
 
     def run(self, tree, seed=None, nthreads=None):
@@ -181,11 +182,12 @@ class RefMC:
 
 
 class RefHeat:
-    """The reference heat MEX (finiteElementHeatPropagator.c) on the host cores."""
+    """The reference heat MEX (finiteElementHeatPropagator.c) on the host cores. With
+    libname="libmex_heat_cuda.so" it drives this library's heat MEX gateway instead."""
 
-    def __init__(self):
+    def __init__(self, libname="libref_heat.so"):
         self.sh = shim()
-        self.lib = C.CDLL(os.path.join(REF_DIR, "libref_heat.so"))
+        self.lib = C.CDLL(os.path.join(REF_DIR, libname))
         self.fn = self.lib.mexFunction
 
     def run(self, T, Omega, params, nthreads=None):
