@@ -220,6 +220,8 @@ def run_ours(args):
                "kernel_ms": mc_ms, "propagation_steps": steps_mc,
                "steps_per_s": steps_mc / (mc_ms / 1e3)},
     }
+    if args.c2:
+        res["mc_batched"] = batched_sweep_measure(dev, args.c2_instances, args.c2_scale)
     if rank == 0:
         if args.cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
@@ -228,6 +230,35 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def batched_sweep_measure(dev, n_inst, scale):
+    """Batched sweep (64 seeded instances, grids 64^3..200x200x150, 450-900 nm, 1e5-1e7 packets
+    log-uniform, Gaussian beams, half with 64 time bins and cyclic x/y boundaries): one batched
+    launch vs the plain kernel launched once per instance."""
+    from mcmatlab_b200 import native
+    models = configs.batched_sweep(n_instances=n_inst, seed=7, photons=(1e5 * scale, 1e7 * scale))
+    ins = [mexargs.prepare_mc(x) for x in models]
+    total = float(sum(x["nPhotonsRequested"] for x in ins))
+    native.mc_run(dict(ins[0], nPhotonsRequested=1e4), device=dev)
+    native.mc_run_batch([dict(x, nPhotonsRequested=1e3) for x in ins[:4]], device=dev)
+    plain_ms = plain_wall = 0.0
+    for x in ins:
+        t0 = time.perf_counter()
+        o = native.mc_run(x, device=dev)
+        plain_wall += time.perf_counter() - t0
+        plain_ms += o["kernelMs"]
+    t0 = time.perf_counter()
+    outs = native.mc_run_batch(ins, device=dev)
+    batch_wall = time.perf_counter() - t0
+    batch_ms = outs[0]["kernelMs"]
+    return {"workload": "%d-instance batched sweep (grids 64^3..200x200x150, 450-900 nm, %.0e-%.0e packets)"
+                        % (n_inst, 1e5 * scale, 1e7 * scale),
+            "packets": total,
+            "batched_packets_per_s": total / (batch_ms / 1e3), "plain_per_instance_packets_per_s": total / (plain_ms / 1e3),
+            "ratio_device": plain_ms / batch_ms,
+            "batched_e2e_packets_per_s": total / batch_wall, "plain_e2e_packets_per_s": total / plain_wall,
+            "ratio_e2e": plain_wall / batch_wall}
 
 
 def reference_setup():
@@ -305,6 +336,9 @@ def main():
     ap.add_argument("--nt", type=int, default=20000, help="DG-ADI time steps per bench step")
     ap.add_argument("--ref-nt", type=int, default=50, help="time steps per bench step of the CPU reference")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-c2", dest="c2", action="store_false", help="skip the batched-sweep measurement")
+    ap.add_argument("--c2-instances", type=int, default=64)
+    ap.add_argument("--c2-scale", type=float, default=1.0, help="photon-count scale of the batched sweep")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -126,8 +126,9 @@ typedef struct mcb_mc_result {
 MCB_API mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_result *result);
 
 /* No counterpart in the reference: runs n independent models (different grids, media,
- * wavelengths, photon counts) in one persistent launch. Results equal n calls of mcb_mc_run
- * up to FP64 summation order. */
+ * wavelengths, photon counts) in one persistent launch. Each model's packets use the random
+ * streams of its own seed, so results equal n calls of mcb_mc_run up to FP64 summation order.
+ * Batched models need fixed launched-packet counts (no timed or collected-count runs). */
 MCB_API mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,
                             mcb_mc_result *const *results);
 

@@ -707,7 +707,10 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     I.key0 = (uint32_t)m->seed;
     I.key1 = (uint32_t)(m->seed >> 32);
     I.ctr2hi = (uint32_t)iL << 16;
-    I.stream = stream;
+    // streams are keyed by the model's seed only, so a model gives the same packets whether it
+    // runs alone or inside a batch (the batch slot is not part of the counter)
+    I.stream = 0;
+    (void)stream;
     I.count = pl.nPackets[iL];
   }
   return MCB_OK;

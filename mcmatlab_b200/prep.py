@@ -27,8 +27,10 @@ CDFSIZE = 201  # +MCmatlab/src/MCmatlab.c:171 (one more than the 200 theta bins 
 
 
 def _nargs(f):
+    """Number of required positional parameters (MATLAB's nargin of a function handle)."""
     try:
-        return len(inspect.signature(f).parameters)
+        return sum(1 for p in inspect.signature(f).parameters.values()
+                   if p.default is inspect.Parameter.empty and p.kind in (p.POSITIONAL_ONLY, p.POSITIONAL_OR_KEYWORD))
     except (TypeError, ValueError):
         return 1
 
@@ -90,26 +92,22 @@ def sobel_gradients(I):
     array dimension. imgradientxyz names its outputs the other way round for the
     first two (its 'Gx' differentiates along columns), which getOpticalMediaProperties.m:229
     undoes by unpacking them as [Gy_Sobel, Gx_Sobel, Gz_Sobel].
+
+    The kernels are central differences [-1 0 1] along the derivative axis times the
+    transverse weights [[1 3 1],[3 6 3],[1 3 1]] = [1 3 1] x [1 3 1] - 3 delta, evaluated
+    with separable 1-D correlations.
     """
+    from scipy.ndimage import correlate1d
     I = np.asarray(I, dtype=np.float64)
-    P = _replicate_pad(I)
-    s = np.array([[1.0, 3.0, 1.0], [3.0, 6.0, 3.0], [1.0, 3.0, 1.0]])  # transverse weights
-    nx, ny, nz = I.shape
-
-    def sl(o0, o1, o2):
-        return P[1 + o0:1 + o0 + nx, 1 + o1:1 + o1 + ny, 1 + o2:1 + o2 + nz]
-
-    Gx = np.zeros_like(I)
-    Gy = np.zeros_like(I)
-    Gz = np.zeros_like(I)
-    for a in (-1, 0, 1):
-        for b in (-1, 0, 1):
-            # derivative along x: weights s over (y, z) offsets
-            w = s[a + 1, b + 1]
-            Gx += w * (sl(1, a, b) - sl(-1, a, b))
-            Gy += w * (sl(a, 1, b) - sl(a, -1, b))
-            Gz += w * (sl(a, b, 1) - sl(a, b, -1))
-    return Gx, Gy, Gz
+    s = np.array([1.0, 3.0, 1.0])
+    d = np.array([-1.0, 0.0, 1.0])
+    out = []
+    for ax in range(3):
+        o1, o2 = [a for a in range(3) if a != ax]
+        D = correlate1d(I, d, axis=ax, mode="nearest")
+        T = correlate1d(correlate1d(D, s, axis=o1, mode="nearest"), s, axis=o2, mode="nearest")
+        out.append(T - 3.0 * D)
+    return out[0], out[1], out[2]
 
 
 def interface_normals(M1, n_per_submedium, dx, dy, dz):
