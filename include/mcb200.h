@@ -132,6 +132,35 @@ MCB_API mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_re
 MCB_API mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,
                             mcb_mc_result *const *results);
 
+/* No counterpart in the reference (which has no derivative code): perturbation Monte Carlo.
+ * Each packet carries its path length L_m and scattering count k_m per medium, which gives the
+ * derivatives of two objectives with respect to every medium's mua and mus in the same run:
+ *   R_b  reflectance (escaping weight per unit area and incident power) on the z < 0 face in
+ *        annuli of width radialBinWidth about (x, y) = (0, 0)       dW/dmua_m = -L_m W,
+ *                                                                  dW/dmus_m = (k_m/mus_m - L_m) W
+ *   F    mean normalised fluence rate over a target voxel box (absorbed weight / mua per
+ *        sub-step, plus the sub-step's own dependence on mua_j)
+ * Requirements: one wavelength, nM <= 10, a fixed packet count, default deposition criteria. */
+typedef struct mcb_mc_objectives {
+  int32_t nRadialBins;     /* 0..64 */
+  double radialBinWidth;   /* [cm] */
+  int32_t box[6];          /* [x0, x1) x [y0, y1) x [z0, z1), 0-based voxel ranges; x1 <= x0: no box */
+} mcb_mc_objectives;
+
+typedef struct mcb_mc_grad_result {
+  double *R;        /* [nRadialBins] [1/cm^2] */
+  double *dR_dmua;  /* [nRadialBins x nM] column-major (bin fastest) [1/cm] */
+  double *dR_dmus;  /* [nRadialBins x nM] */
+  double F;         /* box mean of the normalised fluence rate [1/cm^2] */
+  double *dF_dmua;  /* [nM] */
+  double *dF_dmus;  /* [nM] */
+} mcb_mc_grad_result;
+
+/* Forward transport (outputs as mcb_mc_run, result may hold NULL arrays) plus the objective
+ * values and their per-medium derivatives. */
+MCB_API mcb_status mcb_mc_grad(mcb_ctx *ctx, const mcb_mc_model *model, const mcb_mc_objectives *objectives,
+                               mcb_mc_result *result, mcb_mc_grad_result *grad);
+
 /* ------------------------------------------------------------------------------------------
  * Heat diffusion (Douglas-Gunn ADI) with Arrhenius damage.
  * mcb_heat_params carries the fields of heatSimParameters read by

@@ -63,6 +63,46 @@ class mcb_mc_result(C.Structure):
     ]
 
 
+class mcb_mc_objectives(C.Structure):
+    _fields_ = [("nRadialBins", C.c_int32), ("radialBinWidth", C.c_double), ("box", C.c_int32 * 6)]
+
+
+class mcb_mc_grad_result(C.Structure):
+    _fields_ = [("R", _dp), ("dR_dmua", _dp), ("dR_dmus", _dp), ("F", C.c_double), ("dF_dmua", _dp), ("dF_dmus", _dp)]
+
+
+class GradBuffers:
+    """Objectives and derivative outputs of a perturbation-MC run."""
+
+    def __init__(self, nM, nRadialBins, radialBinWidth, box):
+        self.obj = mcb_mc_objectives()
+        self.obj.nRadialBins = int(nRadialBins)
+        self.obj.radialBinWidth = float(radialBinWidth)
+        for q in range(6):
+            self.obj.box[q] = int(box[q]) if box is not None else 0
+        nR = max(int(nRadialBins), 1)
+        self.R = np.zeros(nR)
+        self.dR_dmua = np.zeros(nR * nM)
+        self.dR_dmus = np.zeros(nR * nM)
+        self.dF_dmua = np.zeros(nM)
+        self.dF_dmus = np.zeros(nM)
+        g = mcb_mc_grad_result()
+        g.R = _ptr(self.R, C.c_double)
+        g.dR_dmua = _ptr(self.dR_dmua, C.c_double)
+        g.dR_dmus = _ptr(self.dR_dmus, C.c_double)
+        g.dF_dmua = _ptr(self.dF_dmua, C.c_double)
+        g.dF_dmus = _ptr(self.dF_dmus, C.c_double)
+        self.res = g
+        self.nR = int(nRadialBins)
+        self.nM = nM
+
+    def outputs(self):
+        nR, nM = self.nR, self.nM
+        return {"R": self.R[:nR].copy(), "dR_dmua": self.dR_dmua[:nR * nM].reshape(nR, nM, order="F"),
+                "dR_dmus": self.dR_dmus[:nR * nM].reshape(nR, nM, order="F"), "F": self.res.F,
+                "dF_dmua": self.dF_dmua.copy(), "dF_dmus": self.dF_dmus.copy()}
+
+
 class mcb_heat_params(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("nM", C.c_int32),

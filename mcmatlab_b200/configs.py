@@ -145,3 +145,47 @@ def batched_sweep(n_instances=64, seed=7, min_grid=(64, 64, 64), max_grid=(200, 
         m.G.updateGeometry()
         out.append(m)
     return out
+
+
+def perturbation_cube(n=256, nPhotons=1e8, seed=11, media_seed=5, L=0.5):
+    """Perturbation-MC workload: an n^3 cube of side L cm with 8 tissue media (6 z-layers and 2
+    ellipsoidal inclusions, seeded mua in [0.1, 50] /cm, mus in [20, 400] /cm, g = 0.9, n = 1.4)
+    under a one-voxel air layer (mua = mus = 1e-8, n = 1) so that light can escape through the
+    top face (MCmatlab counts an escape only where the refractive index is 1). Pencil beam at
+    the centre, all faces escaping."""
+    rng = np.random.default_rng(media_seed)
+    mua = np.exp(rng.uniform(np.log(0.1), np.log(50.0), 8))
+    mus = np.exp(rng.uniform(np.log(20.0), np.log(400.0), 8))
+    bounds = np.sort(rng.uniform(0.05, 0.95, 5)) * L
+    ell = [(rng.uniform(-0.25, 0.25) * L, rng.uniform(-0.25, 0.25) * L, rng.uniform(0.2, 0.7) * L,
+            rng.uniform(0.05, 0.15) * L, rng.uniform(0.05, 0.15) * L, rng.uniform(0.03, 0.1) * L) for _ in range(2)]
+    dz = L / n
+
+    def media(params):
+        out = [mm.mediumProperties(name="air", mua=1e-8, mus=1e-8, g=1.0, n=1.0)]
+        for k in range(8):
+            out.append(mm.mediumProperties(name="tissue%d" % k, mua=float(mua[k]), mus=float(mus[k]), g=0.9, n=1.4))
+        return out
+
+    def geom(X, Y, Z, p):
+        M = np.full(X.shape, 7.0)  # deepest layer; media indices are 1-based (1 = air, 2..9 = tissue0..7)
+        for k in range(5):
+            M[Z < bounds[4 - k]] = 6 - k
+        for q, (cx, cy, cz, ax, ay, az) in enumerate(ell):
+            M[((X - cx) / ax) ** 2 + ((Y - cy) / ay) ** 2 + ((Z - cz) / az) ** 2 < 1] = 8 + q
+        M[Z < dz] = 1
+        return M
+
+    m = mm.model()
+    m.G.nx = m.G.ny = m.G.nz = n
+    m.G.Lx = m.G.Ly = m.G.Lz = L
+    m.G.mediaPropertiesFunc = media
+    m.G.geomFunc = geom
+    m.MC.nPhotonsRequested = nPhotons
+    m.MC.seed = seed
+    m.MC.matchedInterfaces = False
+    m.MC.boundaryType = 1
+    m.MC.wavelength = 700.0
+    m.MC.silentMode = True
+    m.G.updateGeometry()
+    return m

@@ -60,6 +60,28 @@ struct Inst {
   uint32_t key0, key1, ctr2hi, stream;
   // packet range of this instance in the global packet index space
   unsigned long long first, count;
+  // perturbation-MC objectives (gradient runs only)
+  int nR;            // radial reflectance bins on the z < 0 face
+  float rbin;        // bin width [cm]
+  int box[6];        // target box [x0, x1) x [y0, y1) x [z0, z1) for the mean fluence rate
+  double *gR;        // [nR][1 + 2 nM]: value, d/dmua_m, d/dmus_m
+  double *gF;        // [1 + 2 nM]
+};
+
+constexpr int kGradMedia = 10;  // media supported by gradient runs
+
+// Per-packet perturbation-MC state: path length L_m and scattering count k_m per medium.
+// d/dmua of c(mua) = w (1 - exp(-mua s)) / mua is w s^2 phi(mua s) with
+// phi(x) = (exp(-x) - (1 - exp(-x)) / x) / x; its Taylor series -1/2 + x/3 - x^2/8 + x^3/30
+// replaces the cancelling direct form for small x (air has mua = 1e-8 /cm)
+__device__ __forceinline__ float self_phi(float x) {
+  if (x < 0.05f) return -0.5f + x * (1.f / 3.f - x * (0.125f - x * (1.f / 30.f)));
+  return (expf(-x) + expm1f(-x) / x) / x;
+}
+
+struct GradState {
+  float L[kGradMedia];
+  float k[kGradMedia];
 };
 
 struct Photon {
@@ -71,6 +93,8 @@ struct Photon {
   int cdf;
   float stepLeft, weight, time;
   bool inside, alive, sameVoxel;
+  int med;   // medium of the current voxel
+  bool inbox;  // current voxel inside the gradient target box
   uint32_t scat, refr, refl, itr;
   int kec;  // 0 killed, 1 escaped, 2 collected
   // RNG
@@ -178,6 +202,12 @@ __device__ __forceinline__ int voxel_index(const Inst &I, const float *i) {
   return (clamp_coord(i[2], I.n[2]) * I.n[1] + clamp_coord(i[1], I.n[1])) * I.n[0] + clamp_coord(i[0], I.n[0]);
 }
 
+// Voxel of position i inside the gradient target box.
+__device__ __forceinline__ bool in_box(const Inst &I, const float *i) {
+  const int cx = clamp_coord(i[0], I.n[0]), cy = clamp_coord(i[1], I.n[1]), cz = clamp_coord(i[2], I.n[2]);
+  return cx >= I.box[0] && cx < I.box[1] && cy >= I.box[2] && cy < I.box[3] && cz >= I.box[4] && cz < I.box[5];
+}
+
 __device__ __forceinline__ void direction_changed(Photon &P, const Inst &I) {
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -190,6 +220,7 @@ __device__ __forceinline__ void direction_changed(Photon &P, const Inst &I) {
 __device__ __forceinline__ void voxel_props(Photon &P, const Inst &I) {
   P.j = voxel_index(I, P.i);
   const int m = __ldg(I.M0 + P.j);
+  P.med = m;
   const float4 mp = I.med[m];
   P.mua = mp.x;
   P.mus = mp.y;
@@ -204,7 +235,7 @@ __device__ __forceinline__ float launch_time(const Photon &P, const Inst &I, con
 }
 
 // launchPhoton (MCmatlablib.c:519-732). Returns false when 1e6 attempts all land outside.
-__device__ bool launch_packet(Photon &P, const Inst &I) {
+__device__ __forceinline__ bool launch_packet(Photon &P, const Inst &I) {
   P.sameVoxel = false;
   P.weight = 1.f;
   P.kec = 0;
@@ -485,7 +516,7 @@ __device__ __forceinline__ void atomic_add_f64(double *p, double v) { atomicAdd(
 
 // formImage (MCmatlablib.c:737-788)
 // With tally == false only the classification (P.kec) is updated.
-__device__ void form_image(Photon &P, const Inst &I, bool tally) {
+__device__ __forceinline__ void form_image(Photon &P, const Inst &I, bool tally) {
   float U[3];
   to_lc_frame(P.u, I.LCth, I.LCph, U);
   if (!(U[2] < 0)) return;
@@ -538,7 +569,7 @@ __device__ __forceinline__ int face_px(float v, int n) {
   return k;
 }
 
-__device__ void edge_fluxes(const Photon &P, const Inst &I) {
+__device__ __forceinline__ void edge_fluxes(const Photon &P, const Inst &I) {
   const double w = P.weight;
   const int n0 = I.n[0], n1 = I.n[1], n2 = I.n[2];
   if (I.bt == 1) {
@@ -561,7 +592,7 @@ __device__ void edge_fluxes(const Photon &P, const Inst &I) {
 
 // checkEscape (MCmatlablib.c:821-889). `tally` is false while replaying a packet.
 // Returns true when a cyclic wrap teleported the packet.
-__device__ bool check_escape(Photon &P, const Inst &I, bool tally) {
+__device__ __forceinline__ bool check_escape(Photon &P, const Inst &I, bool tally) {
   bool esc = false, teleported = false;
   const float hk = kKillRange / 2.0f;
   switch (I.bt) {

@@ -94,11 +94,17 @@ __device__ __forceinline__ unsigned long long fetch_packet(const KernelArgs &a) 
 }
 
 
-__global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
+// Launch bounds: the plain kernel fits 3 blocks of 256 per SM without spills; the gradient
+// variant carries per-packet path lengths, scattering counts and box partial sums (2 blocks).
+template <bool GRAD>
+__global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs a) {
   // single-instance runs read the instance and its medium table from shared memory
   __shared__ Inst sInst;
   __shared__ float4 sMed[256];
   __shared__ int sCdf[256];
+  __shared__ double sR[GRAD ? 64 * (1 + 2 * kGradMedia) : 1];
+  __shared__ double sF[GRAD ? 1 + 2 * kGradMedia : 1];
+  __shared__ float sInvMus[kGradMedia];
   const bool single = a.nInst == 1;
   if (single) {
     const Inst *g0 = a.insts;
@@ -114,8 +120,24 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
     }
     __syncthreads();
   }
+  int nGM = 0, nGR = 0;
+  if (GRAD) {
+    // gradient runs are single-instance (enforced by the host)
+    nGM = sInst.nM;
+    nGR = sInst.nR;
+    for (int k = threadIdx.x; k < nGR * (1 + 2 * nGM); k += blockDim.x) sR[k] = 0.0;
+    for (int k = threadIdx.x; k < 1 + 2 * nGM; k += blockDim.x) sF[k] = 0.0;
+    for (int k = threadIdx.x; k < nGM; k += blockDim.x) sInvMus[k] = 1.0f / sMed[k].y;
+    __syncthreads();
+  }
   Photon P;
   P.alive = false;
+  P.inbox = false;
+  GradState Gs;
+  // per-thread partial sums of the box objective and its derivatives (flushed once at exit)
+  float boxAcc[GRAD ? 1 + 2 * kGradMedia : 1];
+#pragma unroll
+  for (int q = 0; q < (GRAD ? 1 + 2 * kGradMedia : 1); q++) boxAcc[q] = 0.f;
   const Inst *I = single ? &sInst : a.insts;
   bool replay = false;
   bool started = false;
@@ -166,6 +188,14 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
             voxel_props(P, *I);
             atomicAdd(&I->ctr[0], 1ull);
             started = true;
+            if (GRAD) {
+#pragma unroll
+              for (int m = 0; m < kGradMedia; m++) {
+                Gs.L[m] = 0.f;
+                Gs.k[m] = 0.f;
+              }
+              P.inbox = in_box(*I, P.i);
+            }
           } else {
             atomicAdd(&I->ctr[3], 1ull);
             atomicOr(a.status, 2);
@@ -177,10 +207,36 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
     // 3. one propagation sub-step, then the scattering event if the free path is used up
     if (P.alive) {
       if (P.stepLeft > 0) {
+        const int mj = GRAD ? P.med : 0;
+        const float wpre = GRAD ? P.weight : 0.f;
         const float s = propagate(P, *I);
         steps++;
         const float absorb = -P.weight * expm1f(-P.mua * s);
         P.weight -= absorb;
+        if (GRAD) {
+          // perturbation MC: the box tally c = absorb / mua_j (fluence-rate estimator) depends on
+          // mua through the weight (-L_m c) and through the sub-step itself; on mus through the
+          // score of the sampled path up to the end of this sub-step: k_m / mus_m - L_m, where
+          // k counts the interaction that ends the sub-step when the free path ran out here
+          if (P.inside && P.inbox) {
+            const float mua = P.mua;
+            const float c = absorb / mua;
+            const float dself = wpre * s * s * self_phi(mua * s);
+            const float kself = P.stepLeft > 0 ? 0.f : 1.f;
+            boxAcc[0] += c;
+#pragma unroll
+            for (int m = 0; m < kGradMedia; m++) {
+              if (m < nGM) {
+                const float Lincl = Gs.L[m] + (m == mj ? s : 0.f);
+                const float kincl = Gs.k[m] + (m == mj ? kself : 0.f);
+                boxAcc[1 + m] += -Gs.L[m] * c + (m == mj ? dself : 0.f);
+                boxAcc[1 + kGradMedia + m] += (kincl * sInvMus[m] - Lincl) * c;
+              }
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < kGradMedia; m++) Gs.L[m] += (m == mj ? s : 0.f);
+        }
         if (P.inside && I->NFR) {
           double c = 0.0;
           bool dep = false;
@@ -203,7 +259,28 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
         }
         if (!P.sameVoxel) {
           check_escape(P, *I, !replay);
-          if (P.alive) voxel_props(P, *I);
+          if (GRAD && !P.alive && P.kec != 0 && P.i[2] < 0 && nGR > 0) {
+            // reflectance: escaping weight W on the top face, d/dmua_m = -L_m W,
+            // d/dmus_m = (k_m / mus_m - L_m) W
+            const float x = (P.i[0] - I->n[0] / 2.0f) * I->d[0], y = (P.i[1] - I->n[1] / 2.0f) * I->d[1];
+            const int b = (int)(sqrtf(x * x + y * y) / I->rbin);
+            if (b < nGR) {
+              const float W = P.weight;
+              double *row = sR + b * (1 + 2 * nGM);
+              atomicAdd(row, (double)W);
+#pragma unroll
+              for (int m = 0; m < kGradMedia; m++) {
+                if (m < nGM) {
+                  atomicAdd(row + 1 + m, (double)(-Gs.L[m] * W));
+                  atomicAdd(row + 1 + nGM + m, (double)((Gs.k[m] * sInvMus[m] - Gs.L[m]) * W));
+                }
+              }
+            }
+          }
+          if (P.alive) {
+            voxel_props(P, *I);
+            if (GRAD) P.inbox = in_box(*I, P.i);
+          }
         }
       }
       if (P.alive && !(P.stepLeft > 0)) {
@@ -211,12 +288,36 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
           if (rnd(P, *I) <= kChance) P.weight /= kChance;
           else P.alive = false;
         }
-        if (P.alive) scatter(P, *I);
+        if (P.alive) {
+          if (GRAD) {
+            const int mj = P.med;
+#pragma unroll
+            for (int m = 0; m < kGradMedia; m++) Gs.k[m] += (m == mj ? 1.f : 0.f);
+          }
+          scatter(P, *I);
+        }
       }
     }
   }
   // lanes leave the loop at different times, so each adds its own count
   atomicAdd(a.steps, steps);
+  if (GRAD) {
+    if (nGM > 0 && (I->box[1] > I->box[0])) {
+      atomicAdd(&sF[0], (double)boxAcc[0]);
+#pragma unroll
+      for (int m = 0; m < kGradMedia; m++) {
+        if (m < nGM) {
+          atomicAdd(&sF[1 + m], (double)boxAcc[1 + m]);
+          atomicAdd(&sF[1 + nGM + m], (double)boxAcc[1 + kGradMedia + m]);
+        }
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nGR * (1 + 2 * nGM); k += blockDim.x)
+      if (sR[k] != 0.0) atomicAdd(&sInst.gR[k], sR[k]);
+    for (int k = threadIdx.x; k < 1 + 2 * nGM; k += blockDim.x)
+      if (sF[k] != 0.0) atomicAdd(&sInst.gF[k], sF[k]);
+  }
 }
 
 // (theta, phi) pairs -> unit vectors, as getNormal computes them (MCmatlablib.c:909-918).
@@ -718,7 +819,7 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
 
 mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &insts, bool openEnded,
                             unsigned long long collectTarget, double seconds, unsigned long long *stepsOut,
-                            float *msOut, int *statusOut) {
+                            float *msOut, int *statusOut, bool grad = false) {
   cudaStream_t st = ctx->stream;
   const int n = (int)insts.size();
   std::vector<unsigned long long> first(n + 1, 0);
@@ -747,7 +848,7 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
   a.refillMin = 8;
   if (const char *e = std::getenv("MCB_REFILL_MIN")) a.refillMin = std::max(1, std::min(32, std::atoi(e)));
   int blocksPerSm = 0;
-  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, transport_kernel, 256, 0));
+  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, grad ? transport_kernel<true> : transport_kernel<false>, 256, 0));
   if (blocksPerSm < 1) blocksPerSm = 1;
   const int grid = ctx->num_sms * blocksPerSm;
   if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
@@ -761,7 +862,8 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
     a.deadlineNs = now + (unsigned long long)(seconds * 1e9);
   }
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-  transport_kernel<<<grid, 256, 0, st>>>(a);
+  if (grad) transport_kernel<true><<<grid, 256, 0, st>>>(a);
+  else transport_kernel<false><<<grid, 256, 0, st>>>(a);
   MCB_CUDA(ctx, cudaGetLastError());
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
   unsigned long long tail[3];
@@ -842,11 +944,28 @@ mcb_status finish_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, double *nPhCum, d
 
 }  // namespace
 
-static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *models, mcb_mc_result *const *results) {
+static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *models, mcb_mc_result *const *results,
+                             const mcb_mc_objectives *obj = nullptr, mcb_mc_grad_result *grad = nullptr) {
   using namespace mcb;
   for (int k = 0; k < n; k++) {
     MCB_TRY(validate(ctx, models[k]));
     if (!results[k]) return set_error(ctx, MCB_EINVAL, "result %d is NULL", k);
+  }
+  const bool gradRun = obj != nullptr;
+  if (gradRun) {
+    const mcb_mc_model *m = models[0];
+    if (n != 1) return set_error(ctx, MCB_EINVAL, "gradient runs take one model");
+    if (m->nL != 1) return set_error(ctx, MCB_EINVAL, "gradient runs need a single wavelength");
+    if (m->nM > kGradMedia) return set_error(ctx, MCB_EINVAL, "gradient runs support at most %d media", kGradMedia);
+    if (std::isnan(m->nPhotonsRequested) || m->requestCollectedPhotons)
+      return set_error(ctx, MCB_EINVAL, "gradient runs need a fixed launched-packet count");
+    if (!(m->DC_minScatterings == 0 && std::isinf(m->DC_maxScatterings) && m->DC_minRefractions == 0 &&
+          std::isinf(m->DC_maxRefractions) && m->DC_minReflections == 0 && std::isinf(m->DC_maxReflections) &&
+          m->DC_minInterfaceTransitions == 0 && std::isinf(m->DC_maxInterfaceTransitions) && !m->DC_onlyCollected))
+      return set_error(ctx, MCB_EINVAL, "gradient runs need default deposition criteria");
+    if (obj->nRadialBins < 0 || obj->nRadialBins > 64) return set_error(ctx, MCB_EINVAL, "nRadialBins must be 0..64");
+    if (obj->nRadialBins > 0 && !(obj->radialBinWidth > 0)) return set_error(ctx, MCB_EINVAL, "radialBinWidth must be > 0");
+    if (!grad) return set_error(ctx, MCB_EINVAL, "grad result is NULL");
   }
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t bytes = 1 << 20;
@@ -862,6 +981,26 @@ static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *mod
     plans[k].m = models[k];
     plans[k].r = results[k];
     MCB_TRY(build_plan(ctx, ar, plans[k], (uint32_t)k));
+  }
+  double *gR = nullptr, *gF = nullptr;
+  int nGR = 0, nGM = 0, box[6] = {0, 0, 0, 0, 0, 0};
+  if (gradRun) {
+    const mcb_mc_model *m = models[0];
+    nGM = m->nM;
+    nGR = obj->nRadialBins;
+    const int nn[3] = {m->nx, m->ny, m->nz};
+    for (int q = 0; q < 6; q++) box[q] = std::min(std::max(obj->box[q], 0), nn[q / 2]);
+    gR = ar.take<double>(std::max(1, nGR * (1 + 2 * nGM)));
+    gF = ar.take<double>(1 + 2 * nGM);
+    if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
+    MCB_CUDA(ctx, cudaMemsetAsync(gR, 0, 8 * (size_t)std::max(1, nGR * (1 + 2 * nGM)), ctx->stream));
+    MCB_CUDA(ctx, cudaMemsetAsync(gF, 0, 8 * (size_t)(1 + 2 * nGM), ctx->stream));
+    Inst &I = plans[0].insts[0];
+    I.nR = nGR;
+    I.rbin = (float)obj->radialBinWidth;
+    for (int q = 0; q < 6; q++) I.box[q] = box[q];
+    I.gR = gR;
+    I.gF = gF;
   }
   const bool single = n == 1;
   const mcb_mc_model *m0 = models[0];
@@ -900,7 +1039,7 @@ static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *mod
     std::vector<Inst> all;
     for (auto &pl : plans) all.insert(all.end(), pl.insts.begin(), pl.insts.end());
     const size_t mark = ar.used;
-    MCB_TRY(launch_transport(ctx, ar, all, false, 0, 0.0, &steps, &ms, &status));
+    MCB_TRY(launch_transport(ctx, ar, all, false, 0, 0.0, &steps, &ms, &status, gradRun));
     ar.used = mark;
   }
   for (int k = 0; k < n; k++) {
@@ -945,6 +1084,36 @@ static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *mod
       ar.used = mark2;
     }
   }
+  if (gradRun) {
+    // normalisation as for NI (per unit area) and NFR (per voxel volume), MCmatlablib.c:1193-1243
+    const mcb_mc_model *m = models[0];
+    std::vector<double> hR(std::max(1, nGR * (1 + 2 * nGM))), hF(1 + 2 * nGM);
+    MCB_CUDA(ctx, cudaMemcpy(hR.data(), gR, 8 * hR.size(), cudaMemcpyDeviceToHost));
+    MCB_CUDA(ctx, cudaMemcpy(hF.data(), gF, 8 * hF.size(), cudaMemcpyDeviceToHost));
+    const double power = plans[0].power[0];
+    double nf = results[0]->nPhotons / power;
+    if (plans[0].useS) nf /= power;
+    else if (m->sourceType == 2 && (m->boundaryType == 0 || m->boundaryType == 2)) nf /= kKillRange * kKillRange;
+    if (results[0]->nPhotons == 0) nf = 1.0;
+    const double w = obj->radialBinWidth;
+    for (int b = 0; b < nGR; b++) {
+      const double area = 3.14159265358979323846 * w * w * ((b + 1.0) * (b + 1.0) - (double)b * b);
+      const double sc = 1.0 / (area * nf);
+      const double *row = hR.data() + b * (1 + 2 * nGM);
+      if (grad->R) grad->R[b] = row[0] * sc;
+      for (int q = 0; q < nGM; q++) {
+        if (grad->dR_dmua) grad->dR_dmua[b + nGR * q] = row[1 + q] * sc;
+        if (grad->dR_dmus) grad->dR_dmus[b + nGR * q] = row[1 + nGM + q] * sc;
+      }
+    }
+    const double nbox = (double)std::max(0, box[1] - box[0]) * std::max(0, box[3] - box[2]) * std::max(0, box[5] - box[4]);
+    const double sF = nbox > 0 ? 1.0 / (m->dx * m->dy * m->dz * nf * nbox) : 0.0;
+    grad->F = hF[0] * sF;
+    for (int q = 0; q < nGM; q++) {
+      if (grad->dF_dmua) grad->dF_dmua[q] = hF[1 + q] * sF;
+      if (grad->dF_dmus) grad->dF_dmus[q] = hF[1 + nGM + q] * sF;
+    }
+  }
   if (status & 1) return set_error(ctx, MCB_ECANCELLED, "run cancelled");
   if (status & 2) {
     bool any = false;
@@ -959,6 +1128,15 @@ extern "C" mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc
   const mcb_mc_model *ms[1] = {model};
   mcb_mc_result *rs[1] = {result};
   return run_models(ctx, 1, ms, rs);
+}
+
+extern "C" mcb_status mcb_mc_grad(mcb_ctx *ctx, const mcb_mc_model *model, const mcb_mc_objectives *objectives,
+                                  mcb_mc_result *result, mcb_mc_grad_result *grad) {
+  if (!ctx) return MCB_EINVAL;
+  if (!objectives) return mcb::set_error(ctx, MCB_EINVAL, "objectives is NULL");
+  const mcb_mc_model *ms[1] = {model};
+  mcb_mc_result *rs[1] = {result};
+  return run_models(ctx, 1, ms, rs, objectives, grad);
 }
 
 extern "C" mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,

@@ -24,6 +24,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
           6: "MCB_ELAUNCH"}
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
+           "mcb_mc_grad",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -51,6 +52,8 @@ def lib():
             L.mcb_mc_run.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_result)]
             L.mcb_mc_run_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.POINTER(abi.mcb_mc_model)),
                                            C.POINTER(C.POINTER(abi.mcb_mc_result))]
+            L.mcb_mc_grad.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_objectives),
+                                      C.POINTER(abi.mcb_mc_result), C.POINTER(abi.mcb_mc_grad_result)]
             L.mcb_heat_forward.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
                                            C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
             L.mcb_heat_state_create.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
@@ -89,6 +92,17 @@ def mc_run(mc_in, device=0, example_cap=100000):
     rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0)
     _check(lib().mcb_mc_run(ctx, C.byref(mb.model), C.byref(rb.result)), ctx)
     return rb.outputs()
+
+
+def mc_grad(mc_in, nRadialBins=32, radialBinWidth=0.01, box=None, device=0):
+    """Perturbation-MC run: forward outputs plus R (radial reflectance), F (box mean fluence rate)
+    and their derivatives with respect to every medium's mua and mus."""
+    ctx = context(device)
+    mb = abi.McModelBuffers(mc_in)
+    rb = abi.McResultBuffers(mc_in)
+    gb = abi.GradBuffers(int(np.asarray(mc_in["mua"]).shape[0]), nRadialBins, radialBinWidth, box)
+    _check(lib().mcb_mc_grad(ctx, C.byref(mb.model), C.byref(gb.obj), C.byref(rb.result), C.byref(gb.res)), ctx)
+    return rb.outputs(), gb.outputs()
 
 
 def mc_run_batch(mc_ins, device=0):

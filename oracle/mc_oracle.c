@@ -82,6 +82,11 @@ typedef struct {
   uint32_t stream;
   uint32_t iL;
   int aborting;
+  /* perturbation MC (gradient runs) */
+  int grad, nGM, nR;
+  double rbin;
+  int box[6];
+  double *gR, *gF;
 } orc_mc;
 
 typedef struct {
@@ -101,6 +106,8 @@ typedef struct {
   unsigned long scat, refr, refl, itr;
   int kec; /* 0 killed, 1 escaped, 2 collected */
   unsigned long long steps;
+  double L[10], k[10]; /* path length and scattering count per medium (gradient runs) */
+  int inbox;
 } orc_photon;
 
 static double rnd(const orc_mc *R, orc_photon *P) {
@@ -193,8 +200,16 @@ static long newj(const orc_mc *R, const double *i) {
   return c[2] * R->n[0] * R->n[1] + c[1] * R->n[0] + c[0];
 }
 
+static int box_of(const orc_mc *R, const double *i) {
+  long c[3];
+  for (int k = 0; k < 3; k++) c[k] = i[k] < 0 ? 0 : (i[k] >= R->n[k] ? R->n[k] - 1 : (long)floor(i[k]));
+  return c[0] >= R->box[0] && c[0] < R->box[1] && c[1] >= R->box[2] && c[1] < R->box[3] && c[2] >= R->box[4] &&
+         c[2] < R->box[5];
+}
+
 static void voxel_props(const orc_mc *R, orc_photon *P) {
   P->j = newj(R, P->i);
+  if (R->grad) P->inbox = box_of(R, P->i);
   int m = R->M0[P->j];
   P->mua = R->mua[m];
   P->mus = R->mus[m];
@@ -400,7 +415,16 @@ static void interp_normal(const orc_mc *R, const orc_photon *P, long jn, double 
   nv[2] /= nrm;
 }
 
+/* (e^{-x} - (1 - e^{-x}) / x) / x, by its Taylor series -1/2 + x/3 - x^2/8 + x^3/30 - x^4/144
+ * where the direct form cancels */
+static double self_phi(double x) {
+  if (x < 0.05) return -0.5 + x * (1.0 / 3.0 - x * (0.125 - x * (1.0 / 30.0 - x / 144.0)));
+  return (exp(-x) + expm1(-x) / x) / x;
+}
+
 static void propagate(orc_mc *R, orc_photon *P) {
+  const int mj = R->M0[P->j];
+  const double wpre = P->weight;
   P->sameVoxel = true;
   P->steps++;
   double s = fmin(P->stepLeft / P->mus, fmin(P->D[0], fmin(P->D[1], P->D[2])));
@@ -455,6 +479,23 @@ static void propagate(orc_mc *R, orc_photon *P) {
   }
   double absorb = -P->weight * expm1(-P->mua * s);
   P->weight -= absorb;
+  if (R->grad) {
+    if (P->insideVolume && P->inbox) {
+      /* c(mua) = w (1 - e^{-mua s}) / mua; dc/dmua = w s^2 phi(mua s) (self_phi); the score for
+       * mus counts the interaction that ends this step when the free path ran out here */
+      const double mua = P->mua, c = absorb / mua;
+      const double dself = wpre * s * s * self_phi(mua * s);
+      const double kself = P->stepLeft > 0 ? 0.0 : 1.0;
+      add(&R->gF[0], c);
+      for (int m = 0; m < R->nGM; m++) {
+        const double Lincl = P->L[m] + (m == mj ? s : 0.0);
+        const double kincl = P->k[m] + (m == mj ? kself : 0.0);
+        add(&R->gF[1 + m], -P->L[m] * c + (m == mj ? dself : 0.0));
+        add(&R->gF[1 + R->nGM + m], (kincl / R->mus[m] - Lincl) * c);
+      }
+    }
+    P->L[mj] += s;
+  }
   if (P->insideVolume) {
     if (!R->eol) {
       if (R->NFR && criteria(R, P)) add(&R->NFR[P->j], absorb);
@@ -577,10 +618,24 @@ static void check_escape(orc_mc *R, orc_photon *P) {
     }
   }
   if (!P->alive && R->bt && criteria(R, P)) edge_fluxes(R, P);
+  if (R->grad && !P->alive && P->kec != 0 && P->i[2] < 0 && R->nR > 0) {
+    const double x = (P->i[0] - R->n[0] / 2.0) * R->d[0], y = (P->i[1] - R->n[1] / 2.0) * R->d[1];
+    const long b = (long)(sqrt(x * x + y * y) / R->rbin);
+    if (b < R->nR) {
+      double *row = R->gR + b * (1 + 2 * R->nGM);
+      const double W = P->weight;
+      add(row, W);
+      for (int m = 0; m < R->nGM; m++) {
+        add(row + 1 + m, -P->L[m] * W);
+        add(row + 1 + R->nGM + m, (P->k[m] / R->mus[m] - P->L[m]) * W);
+      }
+    }
+  }
 }
 
 static void scatter(orc_mc *R, orc_photon *P) {
   double ct;
+  if (R->grad) P->k[R->M0[P->j]] += 1.0;
   if (isnan(P->g)) {
     double a = rnd(R, P);
     long jt = bsearch_cdf(a, O_CDFSIZE - 1, R->CDFs + (long)P->CDFidx * O_CDFSIZE);
@@ -617,6 +672,7 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
   P->draw = 0;
   P->bufblock = 0xFFFFFFFFu;
   launch(R, P);
+  for (int m = 0; m < 10; m++) P->L[m] = P->k[m] = 0.0;
   if (P->alive) {
     voxel_props(R, P);
 #pragma omp atomic
@@ -658,10 +714,23 @@ static double *beam_cdf(const mcb_distr *d, int radial, long *L) {
   return o;
 }
 
-/* Runs the whole MEX-equivalent computation. nthreads <= 0: all available. Returns 0 on success. */
-int orc_mc_run(const mcb_mc_model *in, mcb_mc_result *out, int nthreads) {
+/* Runs the whole MEX-equivalent computation; with obj != NULL also the perturbation-MC
+ * objectives and derivatives (one wavelength, nM <= 8). nthreads <= 0: all available. */
+static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads, const mcb_mc_objectives *obj,
+                       mcb_mc_grad_result *gres) {
   orc_mc R;
   memset(&R, 0, sizeof R);
+  if (obj) {
+    if (in->nL != 1 || in->nM > 10) return -2;
+    R.grad = 1;
+    R.nGM = in->nM;
+    R.nR = obj->nRadialBins;
+    R.rbin = obj->radialBinWidth;
+    const long nn[3] = {in->nx, in->ny, in->nz};
+    for (int q = 0; q < 6; q++) R.box[q] = (int)(obj->box[q] < 0 ? 0 : (obj->box[q] > nn[q / 2] ? nn[q / 2] : obj->box[q]));
+    R.gR = (double *)calloc((size_t)(R.nR > 0 ? R.nR : 1) * (1 + 2 * R.nGM), sizeof(double));
+    R.gF = (double *)calloc(1 + 2 * R.nGM, sizeof(double));
+  }
   const long L = (long)in->nx * in->ny * in->nz;
   R.n[0] = in->nx; R.n[1] = in->ny; R.n[2] = in->nz;
   R.d[0] = in->dx; R.d[1] = in->dy; R.d[2] = in->dz;
@@ -861,6 +930,30 @@ int orc_mc_run(const mcb_mc_model *in, mcb_mc_result *out, int nthreads) {
 #undef NORM
     if (R.aborting) break;
   }
+  if (R.grad && gres) {
+    double nf = nPhCum / R.power;
+    if (useS) nf /= R.power;
+    else if (R.beamType == 2 && (R.bt == 0 || R.bt == 2)) nf /= O_KILLRANGE * O_KILLRANGE;
+    for (int b = 0; b < R.nR; b++) {
+      const double area = O_PI * R.rbin * R.rbin * ((b + 1.0) * (b + 1.0) - (double)b * b);
+      const double *row = R.gR + b * (1 + 2 * R.nGM);
+      if (gres->R) gres->R[b] = row[0] / (area * nf);
+      for (int m = 0; m < R.nGM; m++) {
+        if (gres->dR_dmua) gres->dR_dmua[b + R.nR * m] = row[1 + m] / (area * nf);
+        if (gres->dR_dmus) gres->dR_dmus[b + R.nR * m] = row[1 + R.nGM + m] / (area * nf);
+      }
+    }
+    const double nbox = (double)(R.box[1] > R.box[0] ? R.box[1] - R.box[0] : 0) * (R.box[3] > R.box[2] ? R.box[3] - R.box[2] : 0) *
+                        (R.box[5] > R.box[4] ? R.box[5] - R.box[4] : 0);
+    const double sc = nbox > 0 ? 1.0 / (V * nf * nbox) : 0.0;
+    gres->F = R.gF[0] * sc;
+    for (int m = 0; m < R.nGM; m++) {
+      if (gres->dF_dmua) gres->dF_dmua[m] = R.gF[1 + m] * sc;
+      if (gres->dF_dmus) gres->dF_dmus[m] = R.gF[1 + R.nGM + m] * sc;
+    }
+  }
+  free(R.gR);
+  free(R.gF);
   out->nPhotons = nPhCum;
   out->nPhotonsCollected = nColCum;
   out->nThreads = nth;
@@ -873,6 +966,13 @@ int orc_mc_run(const mcb_mc_model *in, mcb_mc_result *out, int nthreads) {
   free(R.NIxp); free(R.NIxn); free(R.NIyp); free(R.NIyn); free(R.NIzp); free(R.NIzn);
   free(S);
   return 0;
+}
+
+int orc_mc_run(const mcb_mc_model *in, mcb_mc_result *out, int nthreads) { return mc_run_impl(in, out, nthreads, NULL, NULL); }
+
+int orc_mc_grad(const mcb_mc_model *in, const mcb_mc_objectives *obj, mcb_mc_result *out, mcb_mc_grad_result *g,
+                int nthreads) {
+  return mc_run_impl(in, out, nthreads, obj, g);
 }
 
 /* Philox known-answer access for tests */

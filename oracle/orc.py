@@ -33,6 +33,9 @@ def lib():
                                    C.POINTER(C.c_float), dp, dp, C.c_int, C.c_int, C.c_long, C.c_double,
                                    dp, dp, C.c_int, dp, dp, dp, dp]
         L.orc_heat_run.restype = C.c_int
+        L.orc_mc_grad.argtypes = [C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_objectives),
+                                  C.POINTER(abi.mcb_mc_result), C.POINTER(abi.mcb_mc_grad_result), C.c_int]
+        L.orc_mc_grad.restype = C.c_int
         L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_lambert_wm1.argtypes = [C.c_double]
         L.orc_lambert_wm1.restype = C.c_double
@@ -57,6 +60,17 @@ def oracle_mc(mc_in, nthreads=0):
     if rc != 0:
         raise RuntimeError("oracle MC run failed (%d)" % rc)
     return rb.outputs()
+
+
+def oracle_mc_grad(mc_in, nRadialBins=32, radialBinWidth=0.01, box=None, nthreads=0):
+    """FP64 perturbation-MC run (same estimator as the GPU) -> (outputs, grad dict)."""
+    mb = abi.McModelBuffers(mc_in)
+    rb = abi.McResultBuffers(mc_in)
+    gb = abi.GradBuffers(int(np.asarray(mc_in["mua"]).shape[0]), nRadialBins, radialBinWidth, box)
+    rc = lib().orc_mc_grad(C.byref(mb.model), C.byref(gb.obj), C.byref(rb.result), C.byref(gb.res), int(nthreads))
+    if rc != 0:
+        raise RuntimeError("oracle gradient run failed (%d)" % rc)
+    return rb.outputs(), gb.outputs()
 
 
 def oracle_heat(T, Omega, hp, nx, ny, nz):
