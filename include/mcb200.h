@@ -201,6 +201,20 @@ MCB_API mcb_status mcb_heat_state_step(mcb_heat_state *state, const mcb_heat_par
 MCB_API mcb_status mcb_heat_state_read(mcb_heat_state *state, float *T, float *Omega);
 MCB_API mcb_status mcb_heat_state_destroy(mcb_heat_state *state);
 
+/* No counterpart in the reference: mcb_heat_forward that allocates no memory, for callers that
+ * cannot allocate at call time (a GPU whose HBM another allocator, e.g. MATLAB's gpuArray pool or
+ * a PyTorch caching allocator, has already reserved; other streams' work that cudaFree's
+ * device-wide synchronisation would stall). Same arguments, outputs and errors as
+ * mcb_heat_forward. Its working set lives in one static 32 MiB device array of the library:
+ * 37 bytes per voxel (29 without damage, 33 with damage but no light) plus 8 per sensor and
+ * step (sensorTemps history) and small per-medium tables; larger problems return MCB_EINVAL
+ * naming the limit. The context comes from mcb_ctx_create, which does allocate: create it
+ * at set-up. The first call on a device performs set-up (cudaGetSymbolAddress of the scratch);
+ * a caller that captures streams makes that first call before capture begins. There is one
+ * scratch per device: calls that overlap in time on the same device race; serialise them. */
+MCB_API mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
+                                           double *sensorTemps, float *maxMediaTemps);
+
 /* No counterpart in the reference: device time in milliseconds (CUDA events on the context's
  * stream) of the transport kernel or stepping loop of the last call on this context. */
 MCB_API double mcb_last_kernel_ms(const mcb_ctx *ctx);

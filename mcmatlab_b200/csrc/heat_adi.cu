@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -862,3 +863,186 @@ extern "C" mcb_status mcb_heat_state_destroy(mcb_heat_state *s) {
 }
 
 extern "C" double mcb_last_kernel_ms(const mcb_ctx *ctx) { return ctx ? ctx->lastKernelMs : 0.0; }
+
+// ---------------------------------------------------------------------------------------------
+// mcb_heat_forward_static: mcb_heat_forward with no device (or host heap) allocation.
+//
+// Who cannot allocate: a host that shares the GPU with an allocator that has already reserved
+// most of HBM (MATLAB's gpuArray pool, a PyTorch caching allocator) sees cudaMalloc fail at call
+// time; and a caller whose other streams keep working on the same device is stalled by the
+// device-wide synchronisation of cudaFree, which the grow-only buffers of mcb_heat_forward
+// perform when the grid changes. This entry instead carves every buffer it needs out of one
+// file-scope __device__ array of kHeatScratchBytes (32 MiB, reserved when the module loads);
+// requests that do not fit are rejected with MCB_EINVAL and a message naming the limit.
+//
+// Zero-initialised state: the per-medium maxima, the step counter and the damage increments
+// must start at zero for every call; the call clears them itself (cudaMemsetAsync) before its
+// first step, and writes every other buffer before reading it, so nothing carries over from a
+// previous call.
+//
+// There is one scratch per device. Calls that overlap in time on the same device (two host
+// threads, or two contexts on one device) share it and race; callers serialise them.
+// The first call on a device performs the set-up: it looks up the scratch's device address
+// with cudaGetSymbolAddress (which may load this file's module) and caches it; a caller that
+// captures streams makes that first call before capture begins.
+// ---------------------------------------------------------------------------------------------
+namespace {
+constexpr size_t kHeatScratchBytes = (size_t)32 << 20;
+constexpr int kScratchDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_heat_scratch[kHeatScratchBytes];
+
+namespace {
+
+std::mutex g_scratch_mu;
+void *g_scratch_ptr[kScratchDevices];
+
+// Device address of g_heat_scratch on the context's device (current device already set).
+mcb_status heat_scratch(mcb_ctx *ctx, void **out) {
+  using namespace mcb;
+  if (ctx->device < 0 || ctx->device >= kScratchDevices)
+    return set_error(ctx, MCB_EINVAL, "mcb_heat_forward_static: device %d out of range", ctx->device);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[ctx->device]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_heat_scratch);
+    if (e != cudaSuccess || !ptr)
+      return set_error(ctx, MCB_ECUDA, "mcb_heat_forward_static: cudaGetSymbolAddress of the scratch failed: %s",
+                       cudaGetErrorString(e));
+    g_scratch_ptr[ctx->device] = ptr;
+  }
+  *out = g_scratch_ptr[ctx->device];
+  return MCB_OK;
+}
+
+// Bump carving of the scratch (256-byte aligned pieces); base == nullptr only measures.
+struct ScratchCarve {
+  char *base;
+  size_t used;
+  void *take(size_t bytes) {
+    void *q = base ? base + used : nullptr;
+    used += (bytes + 255) & ~(size_t)255;
+    return q;
+  }
+};
+
+// Lays the stepper's buffers out in the scratch (or measures them when c.base is null).
+void carve_static_state(ScratchCarve &c, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
+  const long long L = (long long)p->nx * p->ny * p->nz;
+  const int nM = p->nM, nS = p->nSensors;
+  s->T = (float *)c.take(4 * L);
+  s->A = (float *)c.take(4 * L);
+  s->Q = p->lightsOn ? (float *)c.take(4 * L) : nullptr;
+  s->stage = (float *)c.take(4 * (size_t)std::max<long long>(L, nM));
+  s->ib = (float *)c.take(12 * L);
+  s->Om = damage ? (float *)c.take(4 * L) : nullptr;
+  s->dOm = damage ? (float *)c.take(4 * L) : nullptr;
+  s->M = (uint8_t *)c.take(L);
+  s->c = (float *)c.take(12 * (size_t)nM * nM);
+  s->logA = (double *)c.take(8 * (size_t)nM);
+  s->E = (double *)c.take(8 * (size_t)nM);
+  s->maxEnc = (unsigned int *)c.take(4 * (size_t)nM);
+  s->step = (int *)c.take(16);
+  s->sIdx = nS ? (double *)c.take(8 * (size_t)nS) : nullptr;
+  s->sW = nS ? (double *)c.take(24 * (size_t)nS) : nullptr;
+  s->sens = nS ? (double *)c.take(8 * (size_t)nS * (size_t)(p->steps + 1)) : nullptr;
+}
+
+}  // namespace
+
+extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
+                                              double *sensorTemps, float *maxMediaTemps) {
+  using namespace mcb;
+  if (!ctx) return MCB_EINVAL;
+  MCB_TRY(check_params(ctx, p));
+  if (!T || !maxMediaTemps) return set_error(ctx, MCB_EINVAL, "NULL T or maxMediaTemps");
+  if (p->nSensors > 0 && !sensorTemps) return set_error(ctx, MCB_EINVAL, "sensorTemps is NULL");
+  const bool damage = Omega != nullptr;
+  mcb_heat_state s{};  // a view of the scratch; nothing in it is freed
+  ScratchCarve measure{nullptr, 0};
+  carve_static_state(measure, &s, p, damage);
+  if (measure.used > kHeatScratchBytes)
+    return set_error(ctx, MCB_EINVAL,
+                     "mcb_heat_forward_static: this grid needs %zu bytes of device scratch, more than its static "
+                     "limit of %zu bytes (about 37 bytes per voxel plus 8 per sensor and step); use mcb_heat_forward",
+                     measure.used, kHeatScratchBytes);
+  MCB_CUDA(ctx, cudaSetDevice(ctx->device));
+  void *base = nullptr;
+  MCB_TRY(heat_scratch(ctx, &base));
+  ScratchCarve carve{(char *)base, 0};
+  carve_static_state(carve, &s, p, damage);
+  s.ctx = ctx;
+  s.nx = p->nx;
+  s.ny = p->ny;
+  s.nz = p->nz;
+  s.nM = p->nM;
+  s.L = (long long)p->nx * p->ny * p->nz;
+  s.damage = damage;
+  s.tw = std::min(yz_tile_width(p->ny), yz_tile_width(p->nz));
+
+  cudaStream_t st = ctx->stream;
+  const long long L = s.L, nt = p->steps;
+  const int nM = s.nM, nS = p->nSensors;
+  // upload (the same steps as the allocating path; logA is staged on the stack: nM <= 256)
+  double sum = 0.0;
+  for (long long k = 0; k < L; k++) sum += T[k];
+  s.base = sum / (double)L;
+  double logA[256];
+  for (int m = 0; m < nM; m++) logA[m] = std::log(p->A[m]);
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.stage, T, 4 * L, cudaMemcpyHostToDevice, st));
+  to_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s.stage, s.T, s.base, L);
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.M, p->M, L, cudaMemcpyHostToDevice, st));
+  if (s.Q) MCB_CUDA(ctx, cudaMemcpyAsync(s.Q, p->dTdt_abs, 4 * L, cudaMemcpyHostToDevice, st));
+  if (s.Om) MCB_CUDA(ctx, cudaMemcpyAsync(s.Om, Omega, 4 * L, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.c, p->dTdtperdeltaT, 12 * (size_t)nM * nM, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.logA, logA, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.E, p->E, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
+  if (nS) {
+    MCB_CUDA(ctx, cudaMemcpyAsync(s.sIdx, p->tempSensorCornerIdxs, 8 * (size_t)nS, cudaMemcpyHostToDevice, st));
+    MCB_CUDA(ctx, cudaMemcpyAsync(s.sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, st));
+  }
+  // step: factor the line matrices, clear the zero-start state, then plain launches per step
+  HeatDev h = make_dev(&s, p);
+  const int grid = ctx->num_sms * 8;
+  for (int dir = 0; dir < 3; dir++) factor_kernel<<<grid, 128, 0, st>>>(h, dir, s.ib + (size_t)dir * L);
+  MCB_CUDA(ctx, cudaGetLastError());
+  MCB_CUDA(ctx, cudaMemsetAsync(s.maxEnc, 0, 4 * (size_t)nM, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s.step, 0, 16, st));
+  if (s.dOm) MCB_CUDA(ctx, cudaMemsetAsync(s.dOm, 0, 4 * (size_t)L, st));
+  const long long nx = s.nx, ny = s.ny, nz = s.nz;
+  const size_t smemX = x_smem((int)nx);
+  MCB_CUDA(ctx, cudaFuncSetAttribute(pass_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemX));
+  const int tw = s.tw;
+  if (tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
+  else if (tw == 16) MCB_TRY(setup_yz<16>(ctx, (int)ny, (int)nz));
+  else MCB_TRY(setup_yz<8>(ctx, (int)ny, (int)nz));
+  const long long tilesX = ((ny + h.xl - 1) / h.xl) * nz;
+  const int gridX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * 64);
+  const long long tiles = ((nx + tw - 1) / tw) * std::max(ny, nz);
+  const int gridYZ = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 64);
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+  for (long long k = 0; k < nt; k++) {
+    pass_x_kernel<<<gridX, 256, smemX, st>>>(h);
+    if (tw == 32) launch_yz<32>(h, gridYZ, st);
+    else if (tw == 16) launch_yz<16>(h, gridYZ, st);
+    else launch_yz<8>(h, gridYZ, st);
+  }
+  if (nS) final_sensors_kernel<<<1, 128, 0, st>>>(h);
+  if (s.dOm) merge_omega_kernel<<<grid, 256, 0, st>>>(s.Om, s.dOm, L);
+  MCB_CUDA(ctx, cudaGetLastError());
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+  decode_max_kernel<<<1, 256, 0, st>>>(s.maxEnc, s.stage, nM);
+  MCB_CUDA(ctx, cudaMemcpyAsync(maxMediaTemps, s.stage, 4 * (size_t)nM, cudaMemcpyDeviceToHost, st));
+  if (nS) MCB_CUDA(ctx, cudaMemcpyAsync(sensorTemps, s.sens, 8 * (size_t)nS * (nt + 1), cudaMemcpyDeviceToHost, st));
+  // download (after the maxima have left the stage buffer: same-stream order)
+  from_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s.T, s.stage, s.base, L);
+  MCB_CUDA(ctx, cudaMemcpyAsync(T, s.stage, 4 * L, cudaMemcpyDeviceToHost, st));
+  if (s.Om) MCB_CUDA(ctx, cudaMemcpyAsync(Omega, s.Om, 4 * L, cudaMemcpyDeviceToHost, st));
+  MCB_CUDA(ctx, cudaGetLastError());
+  MCB_CUDA(ctx, cudaStreamSynchronize(st));
+  float ms = 0.f;
+  MCB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->lastKernelMs = ms;
+  return MCB_OK;
+}

@@ -24,7 +24,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
           6: "MCB_ELAUNCH"}
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
-           "mcb_mc_grad",
+           "mcb_mc_grad", "mcb_heat_forward_static",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -56,6 +56,8 @@ def lib():
                                       C.POINTER(abi.mcb_mc_result), C.POINTER(abi.mcb_mc_grad_result)]
             L.mcb_heat_forward.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
                                            C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
+            L.mcb_heat_forward_static.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
+                                                  C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
             L.mcb_heat_state_create.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
                                                 C.POINTER(C.c_float), C.POINTER(C.c_void_p)]
             L.mcb_heat_state_step.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_double),
@@ -131,6 +133,24 @@ def heat_forward(T, Omega, hp, nx, ny, nz, device=0):
     _check(lib().mcb_heat_forward(ctx, C.byref(hb.params), Tb.ctypes.data_as(fp),
                                   Ob.ctypes.data_as(fp) if Ob is not None else C.cast(None, fp),
                                   sens.ctypes.data_as(C.POINTER(C.c_double)), mx.ctypes.data_as(fp)), ctx)
+    shp = (nx, ny, nz)
+    return (Tb.reshape(shp, order="F"), None if Ob is None else Ob.reshape(shp, order="F"),
+            sens.reshape(hb.nS, nt + 1, order="F") if hb.nS else np.zeros((0, 0)), mx.reshape(1, -1))
+
+
+def heat_forward_static(T, Omega, hp, nx, ny, nz, device=0):
+    """heat_forward through mcb_heat_forward_static (no allocation; 32 MiB static scratch)."""
+    ctx = context(device)
+    hb = abi.HeatParamBuffers(nx, ny, nz, hp)
+    Tb = np.ascontiguousarray(np.asarray(T, dtype=np.float32).reshape(-1, order="F")).copy()
+    Ob = None if Omega is None else np.ascontiguousarray(np.asarray(Omega, dtype=np.float32).reshape(-1, order="F")).copy()
+    nt = int(hb.params.steps)
+    sens = np.zeros(hb.nS * (nt + 1)) if hb.nS else np.zeros(1)
+    mx = np.zeros(hb.nM, dtype=np.float32)
+    fp = C.POINTER(C.c_float)
+    _check(lib().mcb_heat_forward_static(ctx, C.byref(hb.params), Tb.ctypes.data_as(fp),
+                                         Ob.ctypes.data_as(fp) if Ob is not None else C.cast(None, fp),
+                                         sens.ctypes.data_as(C.POINTER(C.c_double)), mx.ctypes.data_as(fp)), ctx)
     shp = (nx, ny, nz)
     return (Tb.reshape(shp, order="F"), None if Ob is None else Ob.reshape(shp, order="F"),
             sens.reshape(hb.nS, nt + 1, order="F") if hb.nS else np.zeros((0, 0)), mx.reshape(1, -1))
