@@ -10,6 +10,9 @@ No public dataset is involved; each workload is generated from its description:
   TC 0.0037; air VHC 0.0012, TC 0.00026), damage (E = 4.48e5, A = 7.6e66) in the vessel.
 * batched_sweep(...)       — seeded instances of layered media + one cylinder with
   randomised grids, wavelengths and optical properties.
+* perturbation_cube(...)   — 8 seeded tissue media (layers + ellipsoids) under an air layer.
+* heat_adjoint_case(...)   — 4 seeded thermal media, a Gaussian heat-source blob, a damage
+  target ellipsoid and a sparing region (adjoint objectives).
 """
 from __future__ import annotations
 
@@ -189,3 +192,47 @@ def perturbation_cube(n=256, nPhotons=1e8, seed=11, media_seed=5, L=0.5):
     m.MC.silentMode = True
     m.G.updateGeometry()
     return m
+
+
+def heat_adjoint_case(shape=(300, 300, 200), size=(1.0, 1.0, 0.6), nt=2000, seed=21, peak=50.0, dtFactor=0.9,
+                      heatBoundaryType=0, T0=37.0):
+    """Heat-adjoint workload: a grid of `shape` voxels over `size` cm with 4 media (a bulk, a top
+    layer, a deep layer and an ellipsoidal target), seeded TC in [0.002, 0.006] W/cm/K and VHC in
+    [3.0, 4.2] J/cm^3/K, a Gaussian heat-source blob of `peak` W/cm^3 centred on the target, and
+    Arrhenius damage (E = 4.48e5 J/mol, A = 7.6e66 /s) in the target medium. Objectives: damage
+    summed over the target ellipsoid (weight 1 per voxel) and the mean peak temperature over a
+    sparing region (a slab above the target; weight 1/count). dt = dtFactor x the explicit limit.
+
+    Returns dict(T0, hp (heatSimParameters), wd, wp, n, TC, VHC, S (W/cm^3), M1 (1-based), d)."""
+    from . import mexargs, prep
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    Lx, Ly, Lz = size
+    dx, dy, dz = Lx / nx, Ly / ny, Lz / nz
+    x = (np.arange(nx) + 0.5) * dx - Lx / 2
+    y = (np.arange(ny) + 0.5) * dy - Ly / 2
+    z = (np.arange(nz) + 0.5) * dz
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    TC = rng.uniform(0.002, 0.006, 4)
+    VHC = rng.uniform(3.0, 4.2, 4)
+    zt, zd = rng.uniform(0.1, 0.2) * Lz, rng.uniform(0.7, 0.85) * Lz
+    c0 = np.array([rng.uniform(-0.1, 0.1) * Lx, rng.uniform(-0.1, 0.1) * Ly, rng.uniform(0.4, 0.55) * Lz])
+    ax = np.array([rng.uniform(0.08, 0.15) * Lx, rng.uniform(0.08, 0.15) * Ly, rng.uniform(0.08, 0.15) * Lz])
+    M1 = np.ones(shape, dtype=np.uint8)
+    M1[Z < zt] = 2
+    M1[Z > zd] = 3
+    inT = ((X - c0[0]) / ax[0]) ** 2 + ((Y - c0[1]) / ax[1]) ** 2 + ((Z - c0[2]) / ax[2]) ** 2 < 1
+    M1[inT] = 4
+    w = 1.5 * ax
+    S = peak * np.exp(-((X - c0[0]) ** 2 / w[0] ** 2 + (Y - c0[1]) ** 2 / w[1] ** 2 + (Z - c0[2]) ** 2 / w[2] ** 2))
+    c, Q = prep.calc_dTdt_arrays(VHC, TC, dx, dy, dz, S, 1.0, M1)
+    dtmax = prep.calc_dtmax(M1, TC, VHC, dx, dy, dz)
+    A = np.array([0.0, 0.0, 0.0, 7.6e66])
+    E = np.array([0.0, 0.0, 0.0, 4.48e5])
+    hp = mexargs.heat_mex_params(M1, A, E, c, Q, True, heatBoundaryType, None, None, True, nt, dtFactor * dtmax)
+    wd = inT.astype(np.float32)
+    spare = (Z > zt) & (Z < c0[2] - ax[2]) & (np.abs(X - c0[0]) < ax[0]) & (np.abs(Y - c0[1]) < ax[1]) & ~inT
+    wp = np.where(spare, 1.0 / max(int(spare.sum()), 1), 0.0).astype(np.float32)
+    T0a = np.full(shape, T0, dtype=np.float32, order="F")
+    return dict(T0=T0a, hp=hp, wd=np.asfortranarray(wd), wp=np.asfortranarray(wp), n=shape, TC=TC, VHC=VHC,
+                S=S, M1=M1, d=(dx, dy, dz))

@@ -24,48 +24,9 @@
 #include <mutex>
 #include <vector>
 
-#include "internal.h"
+#include "heat_host.h"
 
 namespace mcb {
-
-constexpr double kGasR = 8.3144598;      // finiteElementHeatPropagator.c:86
-constexpr double kCelsiusZero = 273.15;  // finiteElementHeatPropagator.c:87
-
-struct HeatDev {
-  int nx, ny, nz, nM;
-  float *T;        // deviations, in/out
-  float *A;        // intermediate (T1, then T2)
-  const uint8_t *M;
-  const float *c;  // [nM x nM x 3]
-  const float *Q;  // dTdt_abs or nullptr when the light is off
-  const float *ib; // [3][L] inverse pivots
-  float *Omega;    // or nullptr
-  float *dOmega;   // damage accumulated during the current call, or nullptr
-  const double *logA, *E;  // [nM]
-  unsigned int *maxEnc;    // [nM] order-preserving encoded running maxima
-  int hs;          // heat-sinked faces
-  float dt, hdt;
-  double dtd, base;
-  // sensors
-  int nS;
-  const double *sIdx, *sW;  // [nS], [nS x 3]
-  double *sens;             // [nS x (nt+1)]
-  int *stepCounter;
-  int xl;  // x-lines per block in the X pass
-};
-
-__device__ __forceinline__ unsigned int enc_max(float f) {
-  const unsigned int b = __float_as_uint(f);
-  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-
-__device__ __forceinline__ bool sinked(const HeatDev &h, int ix, int iy, int iz) {
-  return h.hs && (ix == 0 || ix == h.nx - 1 || iy == 0 || iy == h.ny - 1 || iz == 0 || iz == h.nz - 1);
-}
-
-__device__ __forceinline__ float cf(const HeatDev &h, int mi, int mj, int dir) {
-  return __ldg(h.c + mi + h.nM * mj + dir * h.nM * h.nM);
-}
 
 // Sensor interpolation (recordTempSensors, finiteElementHeatPropagator.c:652-664) on the
 // current state, written to column `col`.
@@ -82,172 +43,6 @@ __device__ void record_sensors(const HeatDev &h, int col) {
   }
 }
 
-// Tridiagonal line coefficients: a = dt/2 c(M_i, M_prev) couples a row to its predecessor,
-// cc = dt/2 c(M_i, M_next) to its successor; both vanish at the line ends and on heat-sinked
-// rows (identity rows), which reproduces the reference's heat-sink exceptions (:334-349).
-__device__ __forceinline__ bool row_sinked(const HeatDev &h, bool lineSinked, int i, int n) {
-  return lineSinked || (h.hs && (i == 0 || i == n - 1));
-}
-
-// Solves one tridiagonal line with one warp. Shared-memory inputs (element stride st):
-//   rhs  right-hand side, replaced by the solution
-//   fm   forward multipliers  a_i / b'_{i-1}      (Thomas elimination d'_i = rhs_i + fm_i d'_{i-1})
-//   bm   backward multipliers cc_i / b'_i         (back substitution T_i = d'_i / b'_i + bm_i T_{i+1})
-//   ib   inverse pivots 1 / b'_i
-// Each recurrence is evaluated as a chunked warp scan of affine maps: every lane composes the
-// map of its contiguous chunk, a 5-step shuffle scan combines the lanes, and each lane then
-// replays its chunk from the carried-in value.
-__device__ void warp_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
-  const int lane = threadIdx.x & 31;
-  const int k = (n + 31) >> 5;
-  const int s = min(lane * k, n), e = min(s + k, n);
-  float A = 0.f, B = 1.f;
-  for (int i = s; i < e; i++) {
-    const float m = fm[i * st];
-    A = fmaf(m, A, rhs[i * st]);
-    B *= m;
-  }
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const float Au = __shfl_up_sync(0xffffffffu, A, off);
-    const float Bu = __shfl_up_sync(0xffffffffu, B, off);
-    if (lane >= off) {
-      A = fmaf(B, Au, A);
-      B *= Bu;
-    }
-  }
-  float d = __shfl_up_sync(0xffffffffu, A, 1);
-  if (lane == 0) d = 0.f;
-  for (int i = s; i < e; i++) {
-    d = fmaf(fm[i * st], d, rhs[i * st]);
-    rhs[i * st] = d;
-  }
-  A = 0.f;
-  B = 1.f;
-  for (int i = e - 1; i >= s; i--) {
-    const float f = bm[i * st];
-    A = fmaf(f, A, rhs[i * st] * ib[i * st]);
-    B *= f;
-  }
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const float Ad = __shfl_down_sync(0xffffffffu, A, off);
-    const float Bd = __shfl_down_sync(0xffffffffu, B, off);
-    if (lane + off < 32) {
-      A = fmaf(B, Ad, A);
-      B *= Bd;
-    }
-  }
-  float t = __shfl_down_sync(0xffffffffu, A, 1);
-  if (lane == 31) t = 0.f;
-  for (int i = e - 1; i >= s; i--) {
-    t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
-    rhs[i * st] = t;
-  }
-  __syncwarp();
-}
-
-// Grouped variant for short lines: G lanes (an aligned sub-warp group) share one line, each
-// holding K consecutive elements with fully unrolled chunk loops; 32/G lines are solved by a
-// warp at once. Requires n <= G*K.
-template <int K, int G>
-__device__ __forceinline__ void group_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
-  const int g = threadIdx.x & (G - 1);
-  const int kk = (n + G - 1) / G;  // chunk length (<= K); odd lengths spread the lanes over banks
-  const int s = g * kk;
-  const int e = min(s + kk, n);
-  float A = 0.f, B = 1.f;
-#pragma unroll
-  for (int j = 0; j < K; j++) {
-    const int i = s + j;
-    if (i < e) {
-      const float m = fm[i * st];
-      A = fmaf(m, A, rhs[i * st]);
-      B *= m;
-    }
-  }
-#pragma unroll
-  for (int off = 1; off < G; off <<= 1) {
-    const float Au = __shfl_up_sync(0xffffffffu, A, off, G);
-    const float Bu = __shfl_up_sync(0xffffffffu, B, off, G);
-    if (g >= off) {
-      A = fmaf(B, Au, A);
-      B *= Bu;
-    }
-  }
-  float d = __shfl_up_sync(0xffffffffu, A, 1, G);
-  if (g == 0) d = 0.f;
-#pragma unroll
-  for (int j = 0; j < K; j++) {
-    const int i = s + j;
-    if (i < e) {
-      d = fmaf(fm[i * st], d, rhs[i * st]);
-      rhs[i * st] = d;
-    }
-  }
-  A = 0.f;
-  B = 1.f;
-#pragma unroll
-  for (int j = K - 1; j >= 0; j--) {
-    const int i = s + j;
-    if (i < e) {
-      const float f = bm[i * st];
-      A = fmaf(f, A, rhs[i * st] * ib[i * st]);
-      B *= f;
-    }
-  }
-#pragma unroll
-  for (int off = 1; off < G; off <<= 1) {
-    const float Ad = __shfl_down_sync(0xffffffffu, A, off, G);
-    const float Bd = __shfl_down_sync(0xffffffffu, B, off, G);
-    if (g + off < G) {
-      A = fmaf(B, Ad, A);
-      B *= Bd;
-    }
-  }
-  float t = __shfl_down_sync(0xffffffffu, A, 1, G);
-  if (g == G - 1) t = 0.f;
-#pragma unroll
-  for (int j = K - 1; j >= 0; j--) {
-    const int i = s + j;
-    if (i < e) {
-      t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
-      rhs[i * st] = t;
-    }
-  }
-  __syncwarp();
-}
-
-// Lanes per line for the grouped solver (0: use the one-warp-per-line solver).
-__host__ __device__ constexpr int group_lanes(int n) { return n <= 128 ? 8 : (n <= 256 ? 16 : (n <= 512 ? 32 : 0)); }
-
-// Solves `count` lines of one tile; line l starts at base + l*lstride (elements), element
-// stride st. Dispatches on the line length.
-template <int G>
-__device__ __forceinline__ void solve_lines_g(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
-                                              int lstride, int count) {
-  constexpr int LPW = 32 / G;  // lines per warp at once
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int sub = (threadIdx.x & 31) / G;
-  for (int l0 = warp * LPW; l0 < count; l0 += nw * LPW) {
-    const int l = l0 + sub;
-    // groups without a line run the same shuffles on an empty line so the warp stays converged
-    if (l < count) group_solve<16, G>(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
-    else group_solve<16, G>(rhs, fm, bm, ib, 0, st);
-  }
-}
-
-__device__ __forceinline__ void solve_lines(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
-                                            int lstride, int count) {
-  const int G = group_lanes(n);
-  if (G == 8) solve_lines_g<8>(rhs, fm, bm, ib, n, st, lstride, count);
-  else if (G == 16) solve_lines_g<16>(rhs, fm, bm, ib, n, st, lstride, count);
-  else if (G == 32) solve_lines_g<32>(rhs, fm, bm, ib, n, st, lstride, count);
-  else {
-    for (int l = threadIdx.x >> 5; l < count; l += blockDim.x >> 5)
-      warp_solve(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
-  }
-}
 
 // Inverse pivots 1/b'_i of each line's matrix, one thread per line (once per call and dt).
 __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
@@ -592,27 +387,6 @@ mcb_status check_params(mcb_ctx *ctx, const mcb_heat_params *p) {
 
 }  // namespace
 
-// Device-resident stepper state: grids stay in HBM across calls.
-struct mcb_heat_state {
-  mcb_ctx *ctx = nullptr;
-  int nx = 0, ny = 0, nz = 0, nM = 0;
-  long long L = 0;
-  bool damage = false;
-  int tw = 32;
-  double base = 0.0;
-  double factoredDt = -1.0;
-  int factoredHs = -1;
-  float *T = nullptr, *A = nullptr, *Q = nullptr, *ib = nullptr, *Om = nullptr, *dOm = nullptr, *stage = nullptr,
-        *c = nullptr;
-  uint8_t *M = nullptr;
-  double *logA = nullptr, *E = nullptr;
-  unsigned int *maxEnc = nullptr;
-  int *step = nullptr;
-  double *sIdx = nullptr, *sW = nullptr, *sens = nullptr;
-  long long sensCap = 0;
-  int sCap = 0;
-  void *block = nullptr;
-};
 
 namespace {
 
@@ -719,34 +493,12 @@ mcb_status state_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p,
     MCB_CUDA(ctx, cudaMemcpyAsync(s->sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, st));
   }
   if (p->lightsOn && p->dTdt_abs == nullptr) return set_error(ctx, MCB_EINVAL, "dTdt_abs missing while lightsOn");
-  HeatDev h = make_dev(s, p);
+  HeatStepper ks;
+  MCB_TRY(heat_stepper(ctx, s, p, &ks));
+  const HeatDev &h = ks.h;
   const int grid = ctx->num_sms * 8;
-  const long long L = s->L, nx = s->nx, ny = s->ny, nz = s->nz;
-  if (s->factoredDt != p->dt || s->factoredHs != (int)(p->heatBoundaryType != 0)) {
-    for (int dir = 0; dir < 3; dir++) factor_kernel<<<grid, 128, 0, st>>>(h, dir, s->ib + (size_t)dir * L);
-    MCB_CUDA(ctx, cudaGetLastError());
-    s->factoredDt = p->dt;
-    s->factoredHs = (int)(p->heatBoundaryType != 0);
-  }
-  MCB_CUDA(ctx, cudaMemsetAsync(s->maxEnc, 0, 4 * (size_t)s->nM, st));
-  MCB_CUDA(ctx, cudaMemsetAsync(s->step, 0, 16, st));
-  if (s->dOm) MCB_CUDA(ctx, cudaMemsetAsync(s->dOm, 0, 4 * (size_t)L, st));
-  const size_t smemX = x_smem((int)nx);
-  MCB_CUDA(ctx, cudaFuncSetAttribute(pass_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemX));
-  const int tw = s->tw;
-  if (tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
-  else if (tw == 16) MCB_TRY(setup_yz<16>(ctx, (int)ny, (int)nz));
-  else MCB_TRY(setup_yz<8>(ctx, (int)ny, (int)nz));
-  const long long tilesX = ((ny + h.xl - 1) / h.xl) * nz;
-  const int gridX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * 64);
-  const long long tiles = ((nx + tw - 1) / tw) * std::max(ny, nz);
-  const int gridYZ = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 64);
-  auto step = [&](cudaStream_t q) {
-    pass_x_kernel<<<gridX, 256, smemX, q>>>(h);
-    if (tw == 32) launch_yz<32>(h, gridYZ, q);
-    else if (tw == 16) launch_yz<16>(h, gridYZ, q);
-    else launch_yz<8>(h, gridYZ, q);
-  };
+  const long long L = s->L;
+  auto step = [&](cudaStream_t q) { heat_step_launch(ks, q); };
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
   const int chunk = 16;
   if (nt >= chunk) {
@@ -787,6 +539,58 @@ mcb_status state_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Omeg
 }
 
 }  // namespace
+
+namespace mcb {
+
+mcb_status heat_check_params(mcb_ctx *ctx, const mcb_heat_params *p) { return check_params(ctx, p); }
+
+mcb_status heat_state_init(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T,
+                           const float *Omega) {
+  const bool damage = Omega != nullptr;
+  if (!s->block || s->nx != p->nx || s->ny != p->ny || s->nz != p->nz || s->nM != p->nM || s->damage != damage)
+    MCB_TRY(state_alloc(ctx, s, p, damage));
+  return state_upload(ctx, s, p, T, Omega);
+}
+
+void heat_state_release(mcb_heat_state *s) { free_state_buffers(s); }
+
+mcb_status heat_stepper(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, HeatStepper *out) {
+  cudaStream_t st = ctx->stream;
+  HeatStepper &k = *out;
+  k.h = make_dev(s, p);
+  const HeatDev &h = k.h;
+  const int grid = ctx->num_sms * 8;
+  const long long L = s->L, nx = s->nx, ny = s->ny, nz = s->nz;
+  if (s->factoredDt != p->dt || s->factoredHs != (int)(p->heatBoundaryType != 0)) {
+    for (int dir = 0; dir < 3; dir++) factor_kernel<<<grid, 128, 0, st>>>(h, dir, s->ib + (size_t)dir * L);
+    MCB_CUDA(ctx, cudaGetLastError());
+    s->factoredDt = p->dt;
+    s->factoredHs = (int)(p->heatBoundaryType != 0);
+  }
+  MCB_CUDA(ctx, cudaMemsetAsync(s->maxEnc, 0, 4 * (size_t)s->nM, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->step, 0, 16, st));
+  if (s->dOm) MCB_CUDA(ctx, cudaMemsetAsync(s->dOm, 0, 4 * (size_t)L, st));
+  k.smemX = x_smem((int)nx);
+  MCB_CUDA(ctx, cudaFuncSetAttribute(pass_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smemX));
+  k.tw = s->tw;
+  if (k.tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
+  else if (k.tw == 16) MCB_TRY(setup_yz<16>(ctx, (int)ny, (int)nz));
+  else MCB_TRY(setup_yz<8>(ctx, (int)ny, (int)nz));
+  const long long tilesX = ((ny + h.xl - 1) / h.xl) * nz;
+  k.gridX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * 64);
+  const long long tiles = ((nx + k.tw - 1) / k.tw) * std::max(ny, nz);
+  k.gridYZ = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 64);
+  return MCB_OK;
+}
+
+void heat_step_launch(const HeatStepper &k, cudaStream_t q) {
+  pass_x_kernel<<<k.gridX, 256, k.smemX, q>>>(k.h);
+  if (k.tw == 32) launch_yz<32>(k.h, k.gridYZ, q);
+  else if (k.tw == 16) launch_yz<16>(k.h, k.gridYZ, q);
+  else launch_yz<8>(k.h, k.gridYZ, q);
+}
+
+}  // namespace mcb
 
 extern "C" mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega, double *sensorTemps,
                                        float *maxMediaTemps) {

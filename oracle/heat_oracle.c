@@ -158,3 +158,263 @@ int orc_heat_run(long nx, long ny, long nz, int nM, const uint8_t *M, const floa
   free(logA);
   return 0;
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * Adjoint of the DG-ADI step (no counterpart in the reference: it is the checker of the GPU
+ * adjoint). The forward step above, written as linear algebra on the grid vector T:
+ *   D_d   per direction d: (D_d T)_v = sum over the d-neighbours u of v of c(M_v, M_u, d)(T_u - T_v)
+ *         for non-sinked v, 0 for heat-sinked v
+ *   r1 = T + dt (Q + D_x T / 2 + D_y T + D_z T)     A1 = X^-1 r1,  X = I - dt/2 D_x
+ *   r2 = A1 - dt/2 D_y T                             A2 = Y^-1 r2,  Y = I - dt/2 D_y
+ *   r3 = A2 - dt/2 D_z T                             T' = Z^-1 r3,  Z = I - dt/2 D_z
+ *   dOmega_v = dt exp(log A - E / (R ((T_v + T'_v) / 2 + 273.15)))   (media with E != 0)
+ * Objective J = sum_v wd_v sum_n dOmega_v^n + sum_v wp_v max_{n=1..nt} T_v^n. The reverse sweep
+ * carries lambda = dJ/dT^n: rho3 = Z^-T lambda', rho2 = Y^-T rho3, rho1 = X^-T rho2 and
+ *   lambda^n = rho1 + D_x^T (dt/2 rho1) + D_y^T (dt rho1 - dt/2 rho2) + D_z^T (dt rho1 - dt/2 rho3)
+ * plus the damage and peak terms; dJ/dQ = sum_n dt rho1 (non-sinked voxels, light on) and
+ * dJ/dD_d = dt/2 rho1 (T + A1)^T, dt rho1 T^T + dt/2 rho2 (A2 - T)^T, dt rho1 T^T + dt/2 rho3 (T' - T)^T
+ * for d = x, y, z, collected per medium pair onto c. Every state is stored (small grids only).
+ * --------------------------------------------------------------------------------------------- */
+
+typedef struct {
+  long nx, ny, nz, L, sxy;
+  int nM, hs;
+  const uint8_t *M;
+  const double *c;
+  double hdt;
+} adj_grid;
+
+static long dir_stride(const adj_grid *g, int d) { return d == 0 ? 1 : (d == 1 ? g->nx : g->sxy); }
+static long dir_len(const adj_grid *g, int d) { return d == 0 ? g->nx : (d == 1 ? g->ny : g->nz); }
+static long dir_pos(const adj_grid *g, long v, int d) {
+  return d == 0 ? v % g->nx : (d == 1 ? (v / g->nx) % g->ny : v / g->sxy);
+}
+static int vox_sinked(const adj_grid *g, long v) {
+  long ix = v % g->nx, iy = (v / g->nx) % g->ny, iz = v / g->sxy;
+  return sinked(g->hs, ix, iy, iz, g->nx, g->ny, g->nz);
+}
+static double cpair(const adj_grid *g, long v, long u, int d) {
+  return g->c[g->M[v] + g->M[u] * g->nM + d * (long)g->nM * g->nM];
+}
+
+/* out = D_d W (out may not alias W) */
+static void apply_D(const adj_grid *g, int d, const double *W, double *out) {
+  const long st = dir_stride(g, d), n = dir_len(g, d);
+  for (long v = 0; v < g->L; v++) {
+    double s = 0;
+    if (!vox_sinked(g, v)) {
+      long p = dir_pos(g, v, d);
+      if (p > 0) s += cpair(g, v, v - st, d) * (W[v - st] - W[v]);
+      if (p < n - 1) s += cpair(g, v, v + st, d) * (W[v + st] - W[v]);
+    }
+    out[v] = s;
+  }
+}
+
+/* out += D_d^T W */
+static void add_DT(const adj_grid *g, int d, const double *W, double *out) {
+  const long st = dir_stride(g, d), n = dir_len(g, d);
+  for (long v = 0; v < g->L; v++) {
+    if (vox_sinked(g, v)) continue;
+    long p = dir_pos(g, v, d);
+    if (p > 0) {
+      double cc = cpair(g, v, v - st, d);
+      out[v - st] += cc * W[v];
+      out[v] -= cc * W[v];
+    }
+    if (p < n - 1) {
+      double cc = cpair(g, v, v + st, d);
+      out[v + st] += cc * W[v];
+      out[v] -= cc * W[v];
+    }
+  }
+}
+
+/* Solves (I - dt/2 D_d) x = r (transpose = 0) or its transpose (transpose = 1) along every
+ * d-line with the Thomas algorithm on the assembled tridiagonal rows; x may alias r. */
+static void line_solve(const adj_grid *g, int d, int transpose, const double *r, double *x) {
+  const long st = dir_stride(g, d), n = dir_len(g, d);
+  double *sub = (double *)malloc(sizeof(double) * n), *dia = (double *)malloc(sizeof(double) * n);
+  double *sup = (double *)malloc(sizeof(double) * n), *y = (double *)malloc(sizeof(double) * n);
+  for (long v0 = 0; v0 < g->L; v0++) {
+    if (dir_pos(g, v0, d) != 0) continue;
+    for (long p = 0; p < n; p++) {
+      long v = v0 + p * st;
+      sub[p] = sup[p] = 0;
+      dia[p] = 1;
+      if (!vox_sinked(g, v)) {
+        if (p > 0) {
+          sub[p] = -g->hdt * cpair(g, v, v - st, d);
+          dia[p] -= sub[p];
+        }
+        if (p < n - 1) {
+          sup[p] = -g->hdt * cpair(g, v, v + st, d);
+          dia[p] -= sup[p];
+        }
+      }
+      y[p] = r[v];
+    }
+    if (transpose) { /* rows of the transpose: sub'_p = sup_{p-1}, sup'_p = sub_{p+1} */
+      double prev = 0;
+      for (long p = 0; p < n; p++) {
+        double nsub = p > 0 ? prev : 0;
+        prev = sup[p];
+        sup[p] = p < n - 1 ? sub[p + 1] : 0;
+        sub[p] = nsub;
+      }
+    }
+    for (long p = 1; p < n; p++) {
+      double w = sub[p] / dia[p - 1];
+      dia[p] -= w * sup[p - 1];
+      y[p] -= w * y[p - 1];
+    }
+    y[n - 1] /= dia[n - 1];
+    for (long p = n - 2; p >= 0; p--) y[p] = (y[p] - sup[p] * y[p + 1]) / dia[p];
+    for (long p = 0; p < n; p++) x[v0 + p * st] = y[p];
+  }
+  free(sub);
+  free(dia);
+  free(sup);
+  free(y);
+}
+
+static double damage_rate(const adj_grid *g, const double *logA, const double *E, long v, double tmid, double *dRdT) {
+  int m = g->M[v];
+  if (E[m] == 0) {
+    *dRdT = 0;
+    return 0;
+  }
+  double tk = tmid + ORC_CELSIUSZERO;
+  double r = exp(logA[m] - E[m] / (ORC_R * tk));
+  *dRdT = r * E[m] / (ORC_R * tk * tk);
+  return r;
+}
+
+/*
+ * c [nM*nM*3] and Q [L] in double; T0 [L]; wd, wp [L] or NULL. J[0..2] = J, J_damage, J_peak.
+ * dc [nM*nM*3], dQ [L], dT0 [L] may be NULL. Returns 0.
+ */
+int orc_heat_adjoint(long nx, long ny, long nz, int nM, const uint8_t *M, const double *c, const double *Q,
+                     const double *A, const double *E, int lightsOn, int heatSinked, long nt, double dt,
+                     const double *T0, const double *wd, const double *wp, double *J, double *dc, double *dQ,
+                     double *dT0) {
+  adj_grid g = {nx, ny, nz, nx * ny * nz, nx * ny, nM, heatSinked, M, c, dt / 2};
+  const long L = g.L;
+  double *logA = (double *)malloc(sizeof(double) * nM);
+  for (int m = 0; m < nM; m++) logA[m] = log(A[m]);
+  double *Ts = (double *)malloc(sizeof(double) * L * (nt + 1));
+  double *A1s = (double *)malloc(sizeof(double) * L * (nt > 0 ? nt : 1));
+  double *A2s = (double *)malloc(sizeof(double) * L * (nt > 0 ? nt : 1));
+  double *w1 = (double *)malloc(sizeof(double) * L), *w2 = (double *)malloc(sizeof(double) * L);
+  double *pk = (double *)malloc(sizeof(double) * L);
+  long *pkn = (long *)malloc(sizeof(long) * L);
+  memcpy(Ts, T0, sizeof(double) * L);
+  for (long v = 0; v < L; v++) {
+    pk[v] = -INFINITY;
+    pkn[v] = -1;
+  }
+  double Jd = 0, Jp = 0;
+  for (long n = 0; n < nt; n++) {
+    const double *T = Ts + n * L;
+    double *Tn1 = Ts + (n + 1) * L, *A1 = A1s + n * L, *A2 = A2s + n * L;
+    /* r1 */
+    for (long v = 0; v < L; v++) A1[v] = T[v] + (lightsOn && !vox_sinked(&g, v) ? dt * Q[v] : 0);
+    apply_D(&g, 0, T, w1);
+    for (long v = 0; v < L; v++) A1[v] += dt / 2 * w1[v];
+    apply_D(&g, 1, T, w1);
+    apply_D(&g, 2, T, w2);
+    for (long v = 0; v < L; v++) A1[v] += dt * (w1[v] + w2[v]);
+    line_solve(&g, 0, 0, A1, A1);
+    for (long v = 0; v < L; v++) A2[v] = A1[v] - dt / 2 * w1[v];
+    line_solve(&g, 1, 0, A2, A2);
+    for (long v = 0; v < L; v++) Tn1[v] = A2[v] - dt / 2 * w2[v];
+    line_solve(&g, 2, 0, Tn1, Tn1);
+    for (long v = 0; v < L; v++) {
+      double dr;
+      if (wd && wd[v] != 0) Jd += wd[v] * dt * damage_rate(&g, logA, E, v, (T[v] + Tn1[v]) / 2, &dr);
+      if (Tn1[v] > pk[v]) {
+        pk[v] = Tn1[v];
+        pkn[v] = n + 1;
+      }
+    }
+  }
+  if (wp)
+    for (long v = 0; v < L; v++)
+      if (wp[v] != 0) Jp += wp[v] * pk[v];
+  J[0] = Jd + Jp;
+  J[1] = Jd;
+  J[2] = Jp;
+  if (dc || dQ || dT0) {
+    double *lam = (double *)calloc(L, sizeof(double)), *lnew = (double *)malloc(sizeof(double) * L);
+    double *r1 = (double *)malloc(sizeof(double) * L), *r2 = (double *)malloc(sizeof(double) * L);
+    double *r3 = (double *)malloc(sizeof(double) * L), *gd = (double *)malloc(sizeof(double) * L);
+    double *q = (double *)malloc(sizeof(double) * L);
+    if (dc) memset(dc, 0, sizeof(double) * nM * nM * 3);
+    if (dQ) memset(dQ, 0, sizeof(double) * L);
+    for (long n = nt - 1; n >= 0; n--) {
+      const double *T = Ts + n * L, *Tn1 = Ts + (n + 1) * L, *A1 = A1s + n * L, *A2 = A2s + n * L;
+      for (long v = 0; v < L; v++) {
+        double dr = 0;
+        gd[v] = 0;
+        if (wd && wd[v] != 0) {
+          damage_rate(&g, logA, E, v, (T[v] + Tn1[v]) / 2, &dr);
+          gd[v] = wd[v] * dt * dr / 2;
+        }
+        r3[v] = lam[v] + gd[v] + (wp && pkn[v] == n + 1 ? wp[v] : 0);
+      }
+      line_solve(&g, 2, 1, r3, r3);
+      line_solve(&g, 1, 1, r3, r2);
+      line_solve(&g, 0, 1, r2, r1);
+      for (long v = 0; v < L; v++) lnew[v] = r1[v] + gd[v];
+      for (long v = 0; v < L; v++) q[v] = dt / 2 * r1[v];
+      add_DT(&g, 0, q, lnew);
+      for (long v = 0; v < L; v++) q[v] = dt * r1[v] - dt / 2 * r2[v];
+      add_DT(&g, 1, q, lnew);
+      for (long v = 0; v < L; v++) q[v] = dt * r1[v] - dt / 2 * r3[v];
+      add_DT(&g, 2, q, lnew);
+      if (dQ && lightsOn)
+        for (long v = 0; v < L; v++)
+          if (!vox_sinked(&g, v)) dQ[v] += dt * r1[v];
+      if (dc) {
+        for (int d = 0; d < 3; d++) {
+          const long st = dir_stride(&g, d), nl = dir_len(&g, d);
+          for (long v = 0; v < L; v++) {
+            if (vox_sinked(&g, v)) continue;
+            long p = dir_pos(&g, v, d);
+            for (int side = -1; side <= 1; side += 2) {
+              if ((side < 0 && p == 0) || (side > 0 && p == nl - 1)) continue;
+              long u = v + side * st;
+              double contrib;
+              if (d == 0) contrib = dt / 2 * r1[v] * ((T[u] + A1[u]) - (T[v] + A1[v]));
+              else if (d == 1)
+                contrib = dt * r1[v] * (T[u] - T[v]) + dt / 2 * r2[v] * ((A2[u] - T[u]) - (A2[v] - T[v]));
+              else
+                contrib = dt * r1[v] * (T[u] - T[v]) + dt / 2 * r3[v] * ((Tn1[u] - T[u]) - (Tn1[v] - T[v]));
+              dc[M[v] + M[u] * nM + d * (long)nM * nM] += contrib;
+            }
+          }
+        }
+      }
+      double *t = lam;
+      lam = lnew;
+      lnew = t;
+    }
+    if (dT0) memcpy(dT0, lam, sizeof(double) * L);
+    free(lam);
+    free(lnew);
+    free(r1);
+    free(r2);
+    free(r3);
+    free(gd);
+    free(q);
+  }
+  free(logA);
+  free(Ts);
+  free(A1s);
+  free(A2s);
+  free(w1);
+  free(w2);
+  free(pk);
+  free(pkn);
+  return 0;
+}

@@ -5,6 +5,8 @@ and bench.py's CPU-baseline leg.
 
   oracle_mc(mc_in, nthreads)             mc_oracle.c:orc_mc_run on MEX-level inputs
   oracle_heat(T, Omega, heat_params)     heat_oracle.c:orc_heat_run (FP64 DG-ADI)
+  oracle_mc_grad(mc_in, ...)             mc_oracle.c:orc_mc_grad (perturbation MC)
+  oracle_heat_adjoint(T0, hp, ...)       heat_oracle.c:orc_heat_adjoint (FP64 adjoint of the stepper)
 """
 from __future__ import annotations
 
@@ -36,6 +38,10 @@ def lib():
         L.orc_mc_grad.argtypes = [C.POINTER(abi.mcb_mc_model), C.POINTER(abi.mcb_mc_objectives),
                                   C.POINTER(abi.mcb_mc_result), C.POINTER(abi.mcb_mc_grad_result), C.c_int]
         L.orc_mc_grad.restype = C.c_int
+        u8p = C.POINTER(C.c_uint8)
+        L.orc_heat_adjoint.argtypes = [C.c_long, C.c_long, C.c_long, C.c_int, u8p, dp, dp, dp, dp, C.c_int, C.c_int,
+                                       C.c_long, C.c_double, dp, dp, dp, dp, dp, dp, dp]
+        L.orc_heat_adjoint.restype = C.c_int
         L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
         L.orc_lambert_wm1.argtypes = [C.c_double]
         L.orc_lambert_wm1.restype = C.c_double
@@ -91,3 +97,36 @@ def oracle_heat(T, Omega, hp, nx, ny, nz):
     shp = (nx, ny, nz)
     return (Td.reshape(shp, order="F"), None if Od is None else Od.reshape(shp, order="F"),
             None if sens is None else sens.reshape(hb.nS, nt + 1, order="F"), mx)
+
+
+def oracle_heat_adjoint(T0, hp, nx, ny, nz, wd=None, wp=None, c=None, Q=None, grads=True):
+    """FP64 objective J = sum wd * (damage gained) + sum wp * max_n T^n of hp['steps'] DG-ADI steps and,
+    with grads, (J, Jd, Jp), dJ/dc [nM, nM, 3], dJ/dQ and dJ/dT0 (grid shaped). c and Q default to
+    hp's float32 tables and may be given in float64 (finite differences)."""
+    c = np.asarray(hp["dTdtperdeltaT"] if c is None else c, dtype=np.float64)
+    nM = c.shape[0]
+    cd = np.ascontiguousarray(c.reshape(-1, order="F"))
+    Qd = np.ascontiguousarray(np.asarray(hp["dTdt_abs"] if Q is None else Q, dtype=np.float64).reshape(-1, order="F"))
+    M = np.ascontiguousarray(np.asarray(hp["M"], dtype=np.uint8).reshape(-1, order="F"))
+    A = np.ascontiguousarray(np.asarray(hp["A"], dtype=np.float64).ravel())
+    E = np.ascontiguousarray(np.asarray(hp["E"], dtype=np.float64).ravel())
+    T = np.ascontiguousarray(np.asarray(T0, dtype=np.float64).reshape(-1, order="F"))
+    L = T.size
+    dp = C.POINTER(C.c_double)
+    nul = C.cast(None, dp)
+
+    def flat(w):
+        return None if w is None else np.ascontiguousarray(np.asarray(w, dtype=np.float64).reshape(-1, order="F"))
+    wdf, wpf = flat(wd), flat(wp)
+    J = np.zeros(3)
+    dc = np.zeros(nM * nM * 3) if grads else None
+    dQ = np.zeros(L) if grads else None
+    dT = np.zeros(L) if grads else None
+    ptr = lambda a: a.ctypes.data_as(dp) if a is not None else nul
+    lib().orc_heat_adjoint(nx, ny, nz, nM, M.ctypes.data_as(C.POINTER(C.c_uint8)), ptr(cd), ptr(Qd), ptr(A), ptr(E),
+                           int(bool(hp["lightsOn"])), int(hp["heatBoundaryType"]), int(hp["steps"]), float(hp["dt"]),
+                           ptr(T), ptr(wdf), ptr(wpf), ptr(J), ptr(dc), ptr(dQ), ptr(dT))
+    if not grads:
+        return J
+    shp = (nx, ny, nz)
+    return J, dc.reshape(nM, nM, 3, order="F"), dQ.reshape(shp, order="F"), dT.reshape(shp, order="F")
