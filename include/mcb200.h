@@ -201,6 +201,31 @@ MCB_API mcb_status mcb_heat_state_step(mcb_heat_state *state, const mcb_heat_par
 MCB_API mcb_status mcb_heat_state_read(mcb_heat_state *state, float *T, float *Omega);
 MCB_API mcb_status mcb_heat_state_destroy(mcb_heat_state *state);
 
+/* No counterpart in the reference (it has no derivative code): the reverse-time adjoint of the
+ * heat stepper. Runs p->steps steps from T0 (no sensors, no damage state) and returns the
+ * objective
+ *   J = sum_v damageWeight_v * (Arrhenius damage gained by voxel v over the run)
+ *     + sum_v peakWeight_v * max_{n = 1..steps} T_v^n
+ * and its gradients with respect to the conduction table dTdtperdeltaT (c), the heat source
+ * dTdt_abs (Q; zero when the light is off) and the initial temperature. States are checkpointed
+ * every K = ceil(steps / nCheckpoints) steps (nCheckpoints <= 0: ceil(sqrt(steps))) and each
+ * segment is recomputed once during the reverse sweep. At most 32 media. */
+typedef struct {
+  const float *damageWeight; /* [nx*ny*nz] or NULL */
+  const float *peakWeight;   /* [nx*ny*nz] or NULL */
+} mcb_heat_objective;
+
+typedef struct {
+  double J, J_damage, J_peak;  /* out */
+  double *dJ_dc;               /* out [nM x nM x 3], same layout as dTdtperdeltaT, or NULL */
+  float *dJ_dQ;                /* out [nx*ny*nz] or NULL */
+  float *dJ_dT0;               /* out [nx*ny*nz] or NULL */
+  double forwardMs, adjointMs; /* out: device time of the checkpointed forward and of the reverse sweep */
+} mcb_heat_grad;
+
+MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, const float *T0,
+                                    const mcb_heat_objective *objective, int32_t nCheckpoints, mcb_heat_grad *grad);
+
 /* No counterpart in the reference: mcb_heat_forward that allocates no memory, for callers that
  * cannot allocate at call time (a GPU whose HBM another allocator, e.g. MATLAB's gpuArray pool or
  * a PyTorch caching allocator, has already reserved; other streams' work that cudaFree's

@@ -115,6 +115,15 @@ class mcb_heat_params(C.Structure):
     ]
 
 
+class mcb_heat_objective(C.Structure):
+    _fields_ = [("damageWeight", _fp), ("peakWeight", _fp)]
+
+
+class mcb_heat_grad(C.Structure):
+    _fields_ = [("J", C.c_double), ("J_damage", C.c_double), ("J_peak", C.c_double), ("dJ_dc", _dp),
+                ("dJ_dQ", _fp), ("dJ_dT0", _fp), ("forwardMs", C.c_double), ("adjointMs", C.c_double)]
+
+
 def _ptr(a, ctype):
     if a is None:
         return C.cast(None, C.POINTER(ctype))

@@ -1,0 +1,540 @@
+// Reverse-time adjoint of the DG-ADI heat stepper with sqrt(N) checkpointing, behind
+// mcb_heat_adjoint. No counterpart in the reference (finiteElementHeatPropagator.c has no
+// derivative code); the forward it differentiates is the stepper of heat_adi.cu, i.e. the
+// scheme of finiteElementHeatPropagator.c:249-647.
+//
+// One forward step, as linear algebra on the grid (D_d: the conduction operator along d, rows of
+// heat-sinked voxels zero; X, Y, Z = I - dt/2 D_x, D_y, D_z):
+//   A1 = X^-1 (T + dt (Q + D_x T / 2 + D_y T + D_z T))
+//   A2 = Y^-1 (A1 - dt/2 D_y T)
+//   T' = Z^-1 (A2 - dt/2 D_z T)
+// The reverse step takes lambda' = dJ/dT' (plus the objective's terms at T') to
+//   rho3 = Z^-T lambda',  rho2 = Y^-T rho3,  rho1 = X^-T rho2
+//   lambda = rho1 + D_x^T (dt/2 rho1) + D_y^T (dt rho1 - dt/2 rho2) + D_z^T (dt rho1 - dt/2 rho3)
+// and accumulates dJ/dQ += dt rho1 and dJ/dc over the medium pairs of every voxel face.
+//
+// The transposed line solves reuse the forward's inverse pivots: with X = L U (Thomas), the
+// system X^T y = r is the same two first-order recurrences with the multipliers shifted by one
+// row (forward multiplier of row i = cc_{i-1} / b'_{i-1}, backward multiplier = a_{i+1} / b'_i),
+// so the warp-scan solvers of the forward run unchanged. A1 and A2 are not stored by the
+// forward: they follow from T and T' by explicit stencils, A2 = T' - dt/2 D_z (T' - T) and
+// A1 = A2 - dt/2 D_y (A2 - T).
+//
+// Memory: nCheckpoints states of T from the forward sweep, a ring of K + 1 states recomputed
+// per segment (K = ceil(steps / nCheckpoints)), and nine grid-sized work arrays.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "heat_host.h"
+
+namespace mcb {
+namespace {
+
+constexpr int kAdjMaxMedia = 32;
+
+struct AdjDev {
+  HeatDev h;             // grid, media, coefficients, pivots, boundary type, dt
+  const float *Tn, *Tp;  // T^n, T^{n+1} (deviations from the state's base temperature)
+  float *A1, *A2;        // intermediates of step n (reconstructed)
+  float *lam;            // lambda^{n+1}; the objective's terms at T^{n+1} are added in place
+  float *r1, *r2, *r3;   // adjoints of the three solves' right-hand sides
+  float *lamOut;         // lambda^n
+  float *dQ;             // dJ/dQ accumulator, or nullptr (light off or not requested)
+  double *dc;            // [nM x nM x 3] dJ/dc accumulator
+  // objective terms as sparse lists
+  int nD;
+  const int *dIdx;
+  const float *dW;
+  float *gbuf;  // per damage-list entry: d(damage increment)/dT (same for T^n and T^{n+1})
+  double *Jd;
+  int nP;
+  const int *pIdx;
+  const float *pW;
+  const int *pStep;  // step (1..steps) at which each peak-list voxel reached its maximum
+  int step;          // n + 1 of the step being reversed
+};
+
+__device__ __forceinline__ void vox_coords(const HeatDev &h, long long v, int &ix, int &iy, int &iz) {
+  const long long sxy = (long long)h.nx * h.ny;
+  iz = (int)(v / sxy);
+  const long long r = v - (long long)iz * sxy;
+  iy = (int)(r / h.nx);
+  ix = (int)(r - (long long)iy * h.nx);
+}
+
+// out = U - dt/2 D_dir (U - T^n): dir 2 gives A2 from U = T^{n+1}, dir 1 gives A1 from U = A2.
+__global__ void adj_recon_kernel(AdjDev a, int dir) {
+  const HeatDev &h = a.h;
+  const float *U = dir == 2 ? a.Tp : a.A2;
+  float *out = dir == 2 ? a.A2 : a.A1;
+  const long long L = (long long)h.nx * h.ny * h.nz;
+  const long long st = dir == 1 ? h.nx : (long long)h.nx * h.ny;
+  const int n = dir == 1 ? h.ny : h.nz;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    vox_coords(h, v, ix, iy, iz);
+    const int pos = dir == 1 ? iy : iz;
+    const float u = U[v];
+    float d = 0.f;
+    if (!sinked(h, ix, iy, iz)) {
+      const float w = u - a.Tn[v];
+      const int mi = h.M[v];
+      if (pos > 0) d += cf(h, mi, h.M[v - st], dir) * ((U[v - st] - a.Tn[v - st]) - w);
+      if (pos < n - 1) d += cf(h, mi, h.M[v + st], dir) * ((U[v + st] - a.Tn[v + st]) - w);
+    }
+    out[v] = u - h.hdt * d;
+  }
+}
+
+// Objective terms at T^{n+1}: damage (weight w, increment dt A exp(-E / R Tmid)) contributes
+// w dOmega/dT to lambda' (and, kept in gbuf, the same to lambda^n); a peak-list voxel whose
+// maximum was reached at this step contributes its weight.
+__global__ void adj_seed_kernel(AdjDev a) {
+  const HeatDev &h = a.h;
+  double jd = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nD; k += gridDim.x * blockDim.x) {
+    const int v = a.dIdx[k];
+    const int m = h.M[v];
+    float g = 0.f;
+    if (h.E[m] != 0.0) {
+      const double tk = 0.5 * ((double)a.Tn[v] + (double)a.Tp[v]) + h.base + kCelsiusZero;
+      const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tk));
+      const double w = a.dW[k];
+      jd += w * h.dtd * rate;
+      g = (float)(0.5 * w * h.dtd * rate * h.E[m] / (kGasR * tk * tk));
+      atomicAdd(&a.lam[v], g);
+    }
+    a.gbuf[k] = g;
+  }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nP; k += gridDim.x * blockDim.x)
+    if (a.pStep[k] == a.step) atomicAdd(&a.lam[a.pIdx[k]], a.pW[k]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) jd += __shfl_down_sync(0xffffffffu, jd, off);
+  if ((threadIdx.x & 31) == 0 && jd != 0.0) atomicAdd(a.Jd, jd);
+}
+
+__global__ void adj_damage_tail_kernel(AdjDev a) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.nD; k += gridDim.x * blockDim.x)
+    a.lamOut[a.dIdx[k]] += a.gbuf[k];
+}
+
+// X^T solve: rho1 = X^-T rho2. Same tiling as the forward X pass (h.xl lines per block).
+__global__ void __launch_bounds__(256) adj_solve_x_kernel(AdjDev a) {
+  extern __shared__ unsigned char smem[];
+  const HeatDev &h = a.h;
+  const int nx = h.nx, ny = h.ny, nz = h.nz;
+  const int sxy = nx * ny;
+  const int P = nx + 1;
+  const int XL = h.xl;
+  float *rhs = (float *)smem;
+  float *fm = rhs + XL * P;
+  float *bm = fm + XL * P;
+  float *ib = bm + XL * P;
+  const float *ibx = h.ib;
+  const int yTiles = (ny + XL - 1) / XL;
+  for (int tile = blockIdx.x; tile < yTiles * nz; tile += gridDim.x) {
+    const int y0 = (tile % yTiles) * XL, iz = tile / yTiles;
+    const int cnt = min(XL, ny - y0);
+    const int total = cnt * nx;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / nx, x = e - l * nx;
+      const int iy = y0 + l;
+      const int v = x + iy * nx + iz * sxy;
+      const bool lineSinked = h.hs && (iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1);
+      const int mi = h.M[v];
+      const float ibv = ibx[v];
+      float f = 0.f, b = 0.f;
+      if (x > 0 && !row_sinked(h, lineSinked, x - 1, nx)) f = h.hdt * cf(h, h.M[v - 1], mi, 0) * ibx[v - 1];
+      if (x < nx - 1 && !row_sinked(h, lineSinked, x + 1, nx)) b = h.hdt * cf(h, h.M[v + 1], mi, 0) * ibv;
+      rhs[l * P + x] = a.r2[v];
+      fm[l * P + x] = f;
+      bm[l * P + x] = b;
+      ib[l * P + x] = ibv;
+    }
+    __syncthreads();
+    solve_lines(rhs, fm, bm, ib, nx, 1, P, cnt);
+    __syncthreads();
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int l = e / nx, x = e - l * nx;
+      a.r1[x + (y0 + l) * nx + iz * sxy] = rhs[l * P + x];
+    }
+    __syncthreads();
+  }
+}
+
+template <int TW>
+__host__ __device__ constexpr size_t adj_yz_tile_bytes(int n) {
+  return (size_t)n * (4 * (TW + 1) * 4 + TW);
+}
+
+// Y^T / Z^T solves: rho2 = Y^-T rho3 (ZPASS false), rho3 = Z^-T lambda' (ZPASS true). Same
+// tiling as the forward Y/Z passes: TW consecutive x positions, one line per x.
+template <int TW, bool ZPASS>
+__global__ void __launch_bounds__(256) adj_solve_yz_kernel(AdjDev a) {
+  extern __shared__ unsigned char smem[];
+  constexpr int P = TW + 1;
+  const HeatDev &h = a.h;
+  const int nx = h.nx, ny = h.ny, nz = h.nz;
+  const int sxy = nx * ny;
+  const int n = ZPASS ? nz : ny;
+  const int st = ZPASS ? sxy : nx;
+  const int dir = ZPASS ? 2 : 1;
+  float *rhs = (float *)smem;
+  float *ib = rhs + n * P;
+  float *fm = ib + n * P;
+  float *bm = fm + n * P;
+  uint8_t *Ms = (uint8_t *)(bm + n * P);
+  const float *in = ZPASS ? a.lam : a.r3;
+  float *out = ZPASS ? a.r3 : a.r2;
+  const int xTiles = (nx + TW - 1) / TW;
+  const int nOther = ZPASS ? ny : nz;
+  const float *ibd = h.ib + (size_t)dir * sxy * nz;
+  constexpr int RPI = 256 / TW;
+  const int cx = threadIdx.x % TW, r0 = threadIdx.x / TW;
+  for (int tile = blockIdx.x; tile < xTiles * nOther; tile += gridDim.x) {
+    const int x0 = (tile % xTiles) * TW;
+    const int other = tile / xTiles;
+    const int base = ZPASS ? other * nx : other * sxy;
+    const bool otherSinked = h.hs && (other == 0 || other == nOther - 1);
+    const int x = x0 + cx;
+    if (x < nx) {
+      for (int r = r0; r < n; r += RPI) {
+        const int v = base + x + r * st;
+        rhs[r * P + cx] = in[v];
+        ib[r * P + cx] = ibd[v];
+        Ms[r * TW + cx] = h.M[v];
+      }
+    }
+    __syncthreads();
+    if (x < nx) {
+      const bool lineSinked = otherSinked || (h.hs && (x == 0 || x == nx - 1));
+      for (int r = r0; r < n; r += RPI) {
+        const int mi = Ms[r * TW + cx];
+        float f = 0.f, b = 0.f;
+        if (r > 0 && !row_sinked(h, lineSinked, r - 1, n))
+          f = h.hdt * cf(h, Ms[(r - 1) * TW + cx], mi, dir) * ib[(r - 1) * P + cx];
+        if (r < n - 1 && !row_sinked(h, lineSinked, r + 1, n))
+          b = h.hdt * cf(h, Ms[(r + 1) * TW + cx], mi, dir) * ib[r * P + cx];
+        fm[r * P + cx] = f;
+        bm[r * P + cx] = b;
+      }
+    }
+    __syncthreads();
+    solve_lines(rhs, fm, bm, ib, n, P, 1, min(TW, nx - x0));
+    __syncthreads();
+    if (x < nx) {
+      for (int r = r0; r < n; r += RPI) out[base + x + r * st] = rhs[r * P + cx];
+    }
+    __syncthreads();
+  }
+}
+
+// lambda^n, dJ/dQ and dJ/dc of one reversed step (7-point stencil over every voxel).
+__global__ void __launch_bounds__(256) adj_assemble_kernel(AdjDev a) {
+  const HeatDev &h = a.h;
+  __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
+  const int nM = h.nM, nM2 = nM * nM;
+  for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) sdc[k] = 0.0;
+  __syncthreads();
+  const long long L = (long long)h.nx * h.ny * h.nz;
+  const long long sxy = (long long)h.nx * h.ny;
+  const float dt = h.dt, hdt = h.hdt;
+  // same-medium faces (the common case) accumulate in registers, flushed when the medium changes
+  int curM = -1;
+  double same[3] = {0.0, 0.0, 0.0};
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    vox_coords(h, v, ix, iy, iz);
+    const int mv = h.M[v];
+    const bool nsv = !sinked(h, ix, iy, iz);
+    const float r1v = a.r1[v], r2v = a.r2[v], r3v = a.r3[v];
+    const float tv = a.Tn[v];
+    if (nsv && mv != curM) {
+      if (curM >= 0)
+        for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], same[d]);
+      curM = mv;
+      same[0] = same[1] = same[2] = 0.0;
+    }
+    float lam = r1v;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int pos = d == 0 ? ix : (d == 1 ? iy : iz);
+      const int n = d == 0 ? h.nx : (d == 1 ? h.ny : h.nz);
+      const long long st = d == 0 ? 1 : (d == 1 ? h.nx : sxy);
+      const float qv = d == 0 ? hdt * r1v : (d == 1 ? dt * r1v - hdt * r2v : dt * r1v - hdt * r3v);
+      // the field whose face differences carry dJ/dc along d, and its weight at v
+      const float pv = d == 0 ? tv + a.A1[v] : (d == 1 ? a.A2[v] - tv : a.Tp[v] - tv);
+#pragma unroll
+      for (int side = -1; side <= 1; side += 2) {
+        if ((side < 0 && pos == 0) || (side > 0 && pos == n - 1)) continue;
+        const long long u = v + side * st;
+        const int mu = h.M[u];
+        const int ux = d == 0 ? ix + side : ix, uy = d == 1 ? iy + side : iy, uz = d == 2 ? iz + side : iz;
+        if (!sinked(h, ux, uy, uz)) {
+          const float r1u = a.r1[u];
+          const float qu = d == 0 ? hdt * r1u : (d == 1 ? dt * r1u - hdt * a.r2[u] : dt * r1u - hdt * a.r3[u]);
+          lam += cf(h, mu, mv, d) * qu;
+        }
+        if (nsv) {
+          lam -= cf(h, mv, mu, d) * qv;
+          const float tu = a.Tn[u];
+          float contrib;
+          if (d == 0) contrib = hdt * r1v * ((tu + a.A1[u]) - pv);
+          else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((a.A2[u] - tu) - pv);
+          else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((a.Tp[u] - tu) - pv);
+          if (mu == mv) same[d] += (double)contrib;
+          else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
+        }
+      }
+    }
+    a.lamOut[v] = lam;
+    if (a.dQ && nsv) a.dQ[v] += dt * r1v;
+  }
+  if (curM >= 0)
+    for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], same[d]);
+  __syncthreads();
+  for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x)
+    if (sdc[k] != 0.0) atomicAdd(&a.dc[k], sdc[k]);
+}
+
+// Running per-voxel maximum over the peak list after forward step `step`.
+__global__ void peak_track_kernel(const float *T, int nP, const int *idx, float *val, int *at, int step) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nP; k += gridDim.x * blockDim.x) {
+    const float t = T[idx[k]];
+    if (t > val[k]) {
+      val[k] = t;
+      at[k] = step;
+    }
+  }
+}
+
+__global__ void fill_kernel(float *p, float v, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    p[k] = v;
+}
+
+template <int TW>
+mcb_status adj_setup_yz(mcb_ctx *ctx, int ny, int nz) {
+  MCB_CUDA(ctx, cudaFuncSetAttribute(adj_solve_yz_kernel<TW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(adj_yz_tile_bytes<TW>(ny) + 64)));
+  MCB_CUDA(ctx, cudaFuncSetAttribute(adj_solve_yz_kernel<TW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(adj_yz_tile_bytes<TW>(nz) + 64)));
+  return MCB_OK;
+}
+
+template <int TW>
+void adj_launch_yz(const AdjDev &a, bool zpass, int grid, cudaStream_t st) {
+  if (zpass) adj_solve_yz_kernel<TW, true><<<grid, 256, adj_yz_tile_bytes<TW>(a.h.nz) + 64, st>>>(a);
+  else adj_solve_yz_kernel<TW, false><<<grid, 256, adj_yz_tile_bytes<TW>(a.h.ny) + 64, st>>>(a);
+}
+
+// Compressed (index, weight) list of the nonzero entries of a per-voxel weight array.
+void weight_list(const float *w, long long L, std::vector<int> &idx, std::vector<float> &val) {
+  idx.clear();
+  val.clear();
+  if (!w) return;
+  for (long long v = 0; v < L; v++)
+    if (w[v] != 0.f) {
+      idx.push_back((int)v);
+      val.push_back(w[v]);
+    }
+}
+
+}  // namespace
+}  // namespace mcb
+
+extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin, const float *T0,
+                                       const mcb_heat_objective *obj, int32_t nCheckpoints, mcb_heat_grad *out) {
+  using namespace mcb;
+  if (!ctx) return MCB_EINVAL;
+  MCB_TRY(heat_check_params(ctx, pin));
+  if (!T0 || !obj || !out) return set_error(ctx, MCB_EINVAL, "NULL argument");
+  if (pin->steps < 1) return set_error(ctx, MCB_EINVAL, "the adjoint needs steps >= 1");
+  if (pin->nM > kAdjMaxMedia) return set_error(ctx, MCB_EINVAL, "the adjoint supports at most %d media", kAdjMaxMedia);
+  if (pin->lightsOn && !pin->dTdt_abs) return set_error(ctx, MCB_EINVAL, "dTdt_abs missing while lightsOn");
+  mcb_heat_params p = *pin;
+  p.nSensors = 0;  // sensors are not part of the objective
+  p.tempSensorCornerIdxs = p.tempSensorInterpWeights = nullptr;
+  const long long nt = p.steps, L = (long long)p.nx * p.ny * p.nz;
+  const int nM = p.nM;
+  const long long nC = nCheckpoints > 0 ? std::min<long long>(nCheckpoints, nt)
+                                        : (long long)std::ceil(std::sqrt((double)nt));
+  const long long K = (nt + nC - 1) / nC;
+  const long long nSeg = (nt + K - 1) / K;
+  std::vector<int> dIdx, pIdx;
+  std::vector<float> dW, pW;
+  weight_list(obj->damageWeight, L, dIdx, dW);
+  weight_list(obj->peakWeight, L, pIdx, pW);
+  const int nD = (int)dIdx.size(), nP = (int)pIdx.size();
+
+  MCB_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  mcb_heat_state s;
+  s.ctx = ctx;
+  mcb_status rc = heat_state_init(ctx, &s, &p, T0, nullptr);
+  if (rc != MCB_OK) {
+    heat_state_release(&s);
+    return rc;
+  }
+  // work memory: checkpoints, the segment ring, nine grid arrays, the lists and accumulators
+  const size_t grid4 = 4 * (size_t)L;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t bytes = al(grid4) * (size_t)(nSeg + K + 1 + 9) + al(8 * (size_t)nM * nM * 3) + al(16) +
+                       al(12 * (size_t)std::max(nD, 1)) + al(12 * (size_t)std::max(nP, 1)) + al(4 * (size_t)std::max(nP, 1)) +
+                       4096;
+  void *block = nullptr;
+  rc = pool_get(ctx, SLOT_HEAT_ADJ, bytes, &block);
+  if (rc != MCB_OK) {
+    heat_state_release(&s);
+    return rc;
+  }
+  char *cur = (char *)block;
+  auto take = [&](size_t b) {
+    char *q = cur;
+    cur += al(b);
+    return (void *)q;
+  };
+  float *ckpt = (float *)take(grid4 * (size_t)nSeg);
+  float *ring = (float *)take(grid4 * (size_t)(K + 1));
+  AdjDev a{};
+  a.A1 = (float *)take(grid4);
+  a.A2 = (float *)take(grid4);
+  a.r1 = (float *)take(grid4);
+  a.r2 = (float *)take(grid4);
+  a.r3 = (float *)take(grid4);
+  float *lamA = (float *)take(grid4);
+  float *lamB = (float *)take(grid4);
+  float *dQ = (float *)take(grid4);
+  (void)take(grid4);  // spare
+  a.dc = (double *)take(8 * (size_t)nM * nM * 3);
+  a.Jd = (double *)take(16);
+  int *dIdxD = (int *)take(4 * (size_t)std::max(nD, 1));
+  float *dWD = (float *)take(4 * (size_t)std::max(nD, 1));
+  a.gbuf = (float *)take(4 * (size_t)std::max(nD, 1));
+  int *pIdxD = (int *)take(4 * (size_t)std::max(nP, 1));
+  float *pWD = (float *)take(4 * (size_t)std::max(nP, 1));
+  float *pVal = (float *)take(4 * (size_t)std::max(nP, 1));
+  int *pStepD = (int *)take(4 * (size_t)std::max(nP, 1));
+  auto fail = [&](mcb_status r) {
+    heat_state_release(&s);
+    return r;
+  };
+#define ADJ_CUDA(call)                                                                                          \
+  do {                                                                                                          \
+    cudaError_t _e = (call);                                                                                    \
+    if (_e != cudaSuccess)                                                                                      \
+      return fail(set_error(ctx, MCB_ECUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
+                            __LINE__));                                                                         \
+  } while (0)
+  if (nD) {
+    ADJ_CUDA(cudaMemcpyAsync(dIdxD, dIdx.data(), 4 * (size_t)nD, cudaMemcpyHostToDevice, st));
+    ADJ_CUDA(cudaMemcpyAsync(dWD, dW.data(), 4 * (size_t)nD, cudaMemcpyHostToDevice, st));
+  }
+  if (nP) {
+    ADJ_CUDA(cudaMemcpyAsync(pIdxD, pIdx.data(), 4 * (size_t)nP, cudaMemcpyHostToDevice, st));
+    ADJ_CUDA(cudaMemcpyAsync(pWD, pW.data(), 4 * (size_t)nP, cudaMemcpyHostToDevice, st));
+    fill_kernel<<<64, 256, 0, st>>>(pVal, -__builtin_huge_valf(), nP);
+    ADJ_CUDA(cudaMemsetAsync(pStepD, 0, 4 * (size_t)nP, st));
+  }
+  ADJ_CUDA(cudaMemsetAsync(a.dc, 0, 8 * (size_t)nM * nM * 3, st));
+  ADJ_CUDA(cudaMemsetAsync(a.Jd, 0, 16, st));
+  ADJ_CUDA(cudaMemsetAsync(dQ, 0, grid4, st));
+  ADJ_CUDA(cudaMemsetAsync(lamA, 0, grid4, st));
+
+  HeatStepper ks;
+  rc = heat_stepper(ctx, &s, &p, &ks);
+  if (rc != MCB_OK) return fail(rc);
+  a.h = ks.h;
+  a.dQ = p.lightsOn ? dQ : nullptr;
+  a.nD = nD;
+  a.dIdx = dIdxD;
+  a.dW = dWD;
+  a.nP = nP;
+  a.pIdx = pIdxD;
+  a.pW = pWD;
+  a.pStep = pStepD;
+  const int tw = s.tw;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const size_t smemX = (size_t)a.h.xl * 16 * (nx + 1) + 64;
+  ADJ_CUDA(cudaFuncSetAttribute(adj_solve_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemX));
+  if (tw == 32) rc = adj_setup_yz<32>(ctx, ny, nz);
+  else if (tw == 16) rc = adj_setup_yz<16>(ctx, ny, nz);
+  else rc = adj_setup_yz<8>(ctx, ny, nz);
+  if (rc != MCB_OK) return fail(rc);
+  const int gridX = ks.gridX, gridYZ = ks.gridYZ;
+  const int gridE = ctx->num_sms * 8;
+  const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
+
+  // forward sweep: checkpoints every K steps, running maxima of the peak list
+  ADJ_CUDA(cudaEventRecord(ctx->ev0, st));
+  for (long long n = 0; n < nt; n++) {
+    if (n % K == 0) ADJ_CUDA(cudaMemcpyAsync(ckpt + (size_t)(n / K) * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+    heat_step_launch(ks, st);
+    if (nP) peak_track_kernel<<<gridL, 256, 0, st>>>(s.T, nP, pIdxD, pVal, pStepD, (int)(n + 1));
+  }
+  ADJ_CUDA(cudaGetLastError());
+  ADJ_CUDA(cudaEventRecord(ctx->ev1, st));
+  ADJ_CUDA(cudaEventSynchronize(ctx->ev1));
+  float msF = 0.f;
+  ADJ_CUDA(cudaEventElapsedTime(&msF, ctx->ev0, ctx->ev1));
+
+  // reverse sweep, one recomputed segment at a time
+  ADJ_CUDA(cudaEventRecord(ctx->ev0, st));
+  float *lam = lamA, *lamNext = lamB;
+  for (long long seg = nSeg - 1; seg >= 0; seg--) {
+    const long long n0 = seg * K, n1 = std::min(n0 + K, nt);
+    ADJ_CUDA(cudaMemcpyAsync(ring, ckpt + (size_t)seg * L, grid4, cudaMemcpyDeviceToDevice, st));
+    ADJ_CUDA(cudaMemcpyAsync(s.T, ring, grid4, cudaMemcpyDeviceToDevice, st));
+    for (long long j = 1; j <= n1 - n0; j++) {
+      heat_step_launch(ks, st);
+      ADJ_CUDA(cudaMemcpyAsync(ring + (size_t)j * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+    }
+    for (long long n = n1 - 1; n >= n0; n--) {
+      a.Tn = ring + (size_t)(n - n0) * L;
+      a.Tp = ring + (size_t)(n - n0 + 1) * L;
+      a.lam = lam;
+      a.lamOut = lamNext;
+      a.step = (int)(n + 1);
+      if (nD || nP) adj_seed_kernel<<<gridL, 256, 0, st>>>(a);
+      adj_recon_kernel<<<gridE, 256, 0, st>>>(a, 2);
+      adj_recon_kernel<<<gridE, 256, 0, st>>>(a, 1);
+      if (tw == 32) adj_launch_yz<32>(a, true, gridYZ, st);
+      else if (tw == 16) adj_launch_yz<16>(a, true, gridYZ, st);
+      else adj_launch_yz<8>(a, true, gridYZ, st);
+      if (tw == 32) adj_launch_yz<32>(a, false, gridYZ, st);
+      else if (tw == 16) adj_launch_yz<16>(a, false, gridYZ, st);
+      else adj_launch_yz<8>(a, false, gridYZ, st);
+      adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
+      adj_assemble_kernel<<<gridE, 256, 0, st>>>(a);
+      if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
+      std::swap(lam, lamNext);
+    }
+  }
+  ADJ_CUDA(cudaGetLastError());
+  ADJ_CUDA(cudaEventRecord(ctx->ev1, st));
+  // outputs
+  std::vector<float> pv(std::max(nP, 1));
+  double Jd = 0.0;
+  if (nP) ADJ_CUDA(cudaMemcpyAsync(pv.data(), pVal, 4 * (size_t)nP, cudaMemcpyDeviceToHost, st));
+  ADJ_CUDA(cudaMemcpyAsync(&Jd, a.Jd, 8, cudaMemcpyDeviceToHost, st));
+  if (out->dJ_dc) ADJ_CUDA(cudaMemcpyAsync(out->dJ_dc, a.dc, 8 * (size_t)nM * nM * 3, cudaMemcpyDeviceToHost, st));
+  if (out->dJ_dQ) ADJ_CUDA(cudaMemcpyAsync(out->dJ_dQ, dQ, grid4, cudaMemcpyDeviceToHost, st));
+  if (out->dJ_dT0) ADJ_CUDA(cudaMemcpyAsync(out->dJ_dT0, lam, grid4, cudaMemcpyDeviceToHost, st));
+  ADJ_CUDA(cudaStreamSynchronize(st));
+  float msR = 0.f;
+  ADJ_CUDA(cudaEventElapsedTime(&msR, ctx->ev0, ctx->ev1));
+#undef ADJ_CUDA
+  double Jp = 0.0;
+  for (int k = 0; k < nP; k++) Jp += (double)pW[k] * ((double)pv[k] + s.base);
+  out->J_damage = Jd;
+  out->J_peak = Jp;
+  out->J = Jd + Jp;
+  out->forwardMs = msF;
+  out->adjointMs = msR;
+  ctx->lastKernelMs = msF + msR;
+  heat_state_release(&s);
+  return MCB_OK;
+}

@@ -73,6 +73,7 @@ enum PoolSlot {
   SLOT_HEAT_OMEGA,
   SLOT_HEAT_MISC,
   SLOT_HEAT_SENS,
+  SLOT_HEAT_ADJ,
   SLOT_BATCH_BASE = 40
 };
 

@@ -24,7 +24,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
           6: "MCB_ELAUNCH"}
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
-           "mcb_mc_grad", "mcb_heat_forward_static",
+           "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -58,6 +58,8 @@ def lib():
                                            C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
             L.mcb_heat_forward_static.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
                                                   C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
+            L.mcb_heat_adjoint.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
+                                           C.POINTER(abi.mcb_heat_objective), C.c_int32, C.POINTER(abi.mcb_heat_grad)]
             L.mcb_heat_state_create.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_float),
                                                 C.POINTER(C.c_float), C.POINTER(C.c_void_p)]
             L.mcb_heat_state_step.argtypes = [C.c_void_p, C.POINTER(abi.mcb_heat_params), C.POINTER(C.c_double),
@@ -154,6 +156,35 @@ def heat_forward_static(T, Omega, hp, nx, ny, nz, device=0):
     shp = (nx, ny, nz)
     return (Tb.reshape(shp, order="F"), None if Ob is None else Ob.reshape(shp, order="F"),
             sens.reshape(hb.nS, nt + 1, order="F") if hb.nS else np.zeros((0, 0)), mx.reshape(1, -1))
+
+
+def heat_adjoint(T0, hp, nx, ny, nz, damageWeight=None, peakWeight=None, nCheckpoints=0, device=0):
+    """Objective J = sum damageWeight * damage gained + sum peakWeight * max_n T^n over hp['steps'] steps
+    from T0, and its gradients (mcb_heat_adjoint). Returns a dict with J, J_damage, J_peak,
+    dJ_dc [nM, nM, 3], dJ_dQ and dJ_dT0 (grid shaped), forwardMs, adjointMs."""
+    ctx = context(device)
+    hb = abi.HeatParamBuffers(nx, ny, nz, hp)
+    fp = C.POINTER(C.c_float)
+    col = lambda a: None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1, order="F"))
+    Tb, wd, wp = col(T0), col(damageWeight), col(peakWeight)
+    obj = abi.mcb_heat_objective()
+    obj.damageWeight = wd.ctypes.data_as(fp) if wd is not None else C.cast(None, fp)
+    obj.peakWeight = wp.ctypes.data_as(fp) if wp is not None else C.cast(None, fp)
+    nM = hb.nM
+    L = nx * ny * nz
+    dc = np.zeros(nM * nM * 3)
+    dQ = np.zeros(L, dtype=np.float32)
+    dT = np.zeros(L, dtype=np.float32)
+    g = abi.mcb_heat_grad()
+    g.dJ_dc = dc.ctypes.data_as(C.POINTER(C.c_double))
+    g.dJ_dQ = dQ.ctypes.data_as(fp)
+    g.dJ_dT0 = dT.ctypes.data_as(fp)
+    _check(lib().mcb_heat_adjoint(ctx, C.byref(hb.params), Tb.ctypes.data_as(fp), C.byref(obj), int(nCheckpoints),
+                                  C.byref(g)), ctx)
+    shp = (nx, ny, nz)
+    return dict(J=g.J, J_damage=g.J_damage, J_peak=g.J_peak, dJ_dc=dc.reshape(nM, nM, 3, order="F"),
+                dJ_dQ=dQ.reshape(shp, order="F"), dJ_dT0=dT.reshape(shp, order="F"),
+                forwardMs=g.forwardMs, adjointMs=g.adjointMs)
 
 
 def last_kernel_ms(device=0):

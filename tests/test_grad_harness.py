@@ -1,0 +1,81 @@
+"""The torch gradient harness: thermal_tables restates prep.calc_dTdt_arrays (CPU), and on the
+GPU the chained gradients dJ/dTC, dJ/dVHC, dJ/dS (adjoint + torch chain rule) agree with FP64
+central differences of the oracle's objective; ReflectanceFluence returns mcb_mc_grad's values
+and contracts its derivatives."""
+import numpy as np
+import pytest
+import torch
+
+from mcmatlab_b200 import configs, grad, prep
+
+
+def _small():
+    return configs.heat_adjoint_case(shape=(12, 10, 8), size=(0.12, 0.1, 0.08), nt=12, peak=2000.0)
+
+
+def test_thermal_tables_restate_calc_dTdt_arrays():
+    case = _small()
+    c32, Q32 = prep.calc_dTdt_arrays(case["VHC"], case["TC"], *case["d"], case["S"], 1.0, case["M1"])
+    c, Q = grad.thermal_tables(torch.tensor(case["TC"]), torch.tensor(case["VHC"]), torch.tensor(case["S"]),
+                               case["M1"], case["d"])
+    np.testing.assert_allclose(c.numpy(), c32, rtol=2e-6)
+    np.testing.assert_allclose(Q.numpy(), Q32, rtol=2e-6, atol=1e-30)
+
+
+@pytest.mark.gpu
+def test_heat_harness_chain_rule_matches_fp64_differences(oracle_lib):
+    from oracle import orc
+    case = _small()
+    nx, ny, nz = case["n"]
+    TC = torch.tensor(case["TC"], requires_grad=True)
+    VHC = torch.tensor(case["VHC"], requires_grad=True)
+    S = torch.tensor(case["S"], requires_grad=True)
+    c, Q = grad.thermal_tables(TC, VHC, S, case["M1"], case["d"])
+    J = grad.HeatObjective.apply(c, Q, torch.tensor(case["T0"]), case["hp"], case["n"], case["wd"], case["wp"])
+    J.backward()
+
+    def Jref(TCv, VHCv, Sv):
+        cc, QQ = grad.thermal_tables(torch.tensor(TCv), torch.tensor(VHCv), torch.tensor(Sv), case["M1"], case["d"])
+        return orc.oracle_heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"],
+                                       c=cc.numpy(), Q=QQ.numpy(), grads=False)[0]
+
+    h = 1e-5
+    for name, t in (("TC", TC), ("VHC", VHC)):
+        g = t.grad.numpy()
+        for m in range(4):
+            args = [case["TC"].copy(), case["VHC"].copy(), case["S"]]
+            k = 0 if name == "TC" else 1
+            args[k][m] *= 1 + h
+            Jp = Jref(*args)
+            args[k][m] /= 1 + h
+            args[k][m] *= 1 - h
+            Jm = Jref(*args)
+            fd = (Jp - Jm) / (2 * h * [case["TC"], case["VHC"]][k][m])
+            assert abs(g[m] - fd) <= 3e-3 * np.max(np.abs(g)), (name, m, g[m], fd)
+    gS = S.grad.numpy()
+    v = np.unravel_index(np.argmax(np.abs(gS)), gS.shape)
+    Sp, Sm = case["S"].copy(), case["S"].copy()
+    Sp[v] += 1.0
+    Sm[v] -= 1.0
+    fd = (Jref(case["TC"], case["VHC"], Sp) - Jref(case["TC"], case["VHC"], Sm)) / 2.0
+    assert abs(gS[v] - fd) <= 3e-3 * abs(fd)
+
+
+@pytest.mark.gpu
+def test_mc_harness_contracts_perturbation_derivatives():
+    import gradcase
+    from mcmatlab_b200 import native
+    mc_in, obj = gradcase.case(n=24, nPhotons=2e4)
+    mua = torch.tensor(np.asarray(mc_in["mua"])[:, 0], requires_grad=True)
+    mus = torch.tensor(np.asarray(mc_in["mus"])[:, 0], requires_grad=True)
+    R, F = grad.ReflectanceFluence.apply(mua, mus, mc_in, obj)
+    wR = torch.linspace(1.0, 2.0, R.numel(), dtype=torch.float64)
+    (wR @ R + 3.0 * F).backward()
+    _, g = native.mc_grad(mc_in, **obj)
+    # two runs on the same streams: packets land on different threads, so FP32 per-thread box sums
+    # round differently (relative ~1e-6)
+    np.testing.assert_allclose(R.detach().numpy(), g["R"], rtol=1e-5)
+    ga = wR.numpy() @ g["dR_dmua"] + 3.0 * g["dF_dmua"]
+    gs = wR.numpy() @ g["dR_dmus"] + 3.0 * g["dF_dmus"]
+    np.testing.assert_allclose(mua.grad.numpy(), ga, rtol=1e-4, atol=1e-4 * np.max(np.abs(ga)))
+    np.testing.assert_allclose(mus.grad.numpy(), gs, rtol=1e-4, atol=1e-4 * np.max(np.abs(gs)))

@@ -60,3 +60,41 @@ def test_oracle_adjoint_forward_restates_forward_oracle(oracle_lib):
     assert J[1] > 0
     assert abs(J[1] - float((case["wd"] * Om).sum())) <= 1e-12 * J[1]
     assert J[0] == J[1] + J[2]
+
+
+def test_oracle_adjoint_matches_reference_stepper_differences(oracle_lib, ref_available):
+    """Central differences of the reference's own FP32 stepper (damage objective) against the
+    oracle adjoint: agreement within the FP32 difference noise."""
+    if not ref_available:
+        pytest.skip("reference build not present")
+    from oracle import orc, ref
+    case = _case()
+    nx, ny, nz = case["n"]
+    hp, wd = case["hp"], case["wd"]
+    _, dc, dQ, _ = orc.oracle_heat_adjoint(case["T0"], hp, nx, ny, nz, wd, None)
+    rh = ref.RefHeat()
+
+    def Jref(c=None, Q=None):
+        p = dict(hp)
+        if c is not None:
+            p["dTdtperdeltaT"] = np.asfortranarray(c.astype(np.float32))
+        if Q is not None:
+            p["dTdt_abs"] = np.asfortranarray(Q.astype(np.float32))
+        _, Om, _, _ = rh.run(case["T0"], np.zeros(case["n"], np.float32), p, nthreads=1)
+        return float((wd.astype(np.float64) * Om.astype(np.float64)).sum())
+
+    c = np.asarray(hp["dTdtperdeltaT"], dtype=np.float64)
+    h = 2e-2
+    for idx in [(0, 0, 2), (3, 3, 0), (3, 0, 1)]:
+        cp, cm = c.copy(), c.copy()
+        cp[idx] *= 1 + h
+        cm[idx] *= 1 - h
+        fd = (Jref(c=cp) - Jref(c=cm)) / (2 * h * c[idx])
+        assert abs(fd - dc[idx]) <= 2e-2 * np.max(np.abs(dc)), (idx, fd, dc[idx])
+    Q = np.asarray(hp["dTdt_abs"], dtype=np.float64)
+    v = np.unravel_index(np.argmax(np.abs(dQ)), dQ.shape)
+    Qp, Qm = Q.copy(), Q.copy()
+    Qp[v] *= 1 + h
+    Qm[v] *= 1 - h
+    fd = (Jref(Q=Qp) - Jref(Q=Qm)) / (2 * h * Q[v])
+    assert abs(fd - dQ[v]) <= 2e-2 * abs(dQ[v]), (fd, dQ[v])
