@@ -102,6 +102,11 @@ typedef struct mcb_mc_model {
   double DC_minReflections, DC_maxReflections, DC_minInterfaceTransitions, DC_maxInterfaceTransitions;
   double DC_minSubmediaIdx, DC_maxSubmediaIdx; /* 1-based */
   int32_t DC_onlyCollected, DC_evaluateOnlyAtEndOfLife;
+  /* Sharding (no counterpart in the reference): packet k of this run uses the random stream of
+   * packet index packetOffset + k * packetStride (packetStride 0 means 1). Shards r = 0..W-1 of
+   * one seed with offset r and stride W partition the packets of the unsharded run. Example paths
+   * always replay packets 0, 1, 2, ... of the unsharded stream. */
+  uint64_t packetOffset, packetStride;
 } mcb_mc_model;
 
 typedef struct mcb_mc_result {

@@ -48,6 +48,7 @@ class mcb_mc_model(C.Structure):
         ("DC_minInterfaceTransitions", C.c_double), ("DC_maxInterfaceTransitions", C.c_double),
         ("DC_minSubmediaIdx", C.c_double), ("DC_maxSubmediaIdx", C.c_double),
         ("DC_onlyCollected", C.c_int32), ("DC_evaluateOnlyAtEndOfLife", C.c_int32),
+        ("packetOffset", C.c_uint64), ("packetStride", C.c_uint64),
     ]
 
 
@@ -205,6 +206,8 @@ class McModelBuffers:
             setattr(m, "DC_" + k, float(DC[k]))
         m.DC_onlyCollected = int(DC["onlyCollected"])
         m.DC_evaluateOnlyAtEndOfLife = int(DC["evaluateOnlyAtEndOfLife"])
+        m.packetOffset = int(mc_in.get("packetOffset", 0))
+        m.packetStride = int(mc_in.get("packetStride", 1))
         self.model = m
         self.mc_in = mc_in
 

@@ -60,6 +60,8 @@ struct Inst {
   uint32_t key0, key1, ctr2hi, stream;
   // packet range of this instance in the global packet index space
   unsigned long long first, count;
+  // packet k of this instance runs the stream of packet index pOff + k * pStride (sharding)
+  unsigned long long pOff, pStride;
   // perturbation-MC objectives (gradient runs only)
   int nR;            // radial reflectance bins on the z < 0 face
   float rbin;        // bin width [cm]

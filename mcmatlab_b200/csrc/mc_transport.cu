@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
           const int ii = single ? 0 : find_instance(a, g);
           if (!single) I = a.insts + ii;
           pid = g - (single ? 0ull : __ldg(a.instFirst + ii));
+          pid = I->pOff + I->pStride * pid;
           P.pidlo = (uint32_t)pid;
           P.pidhi = (uint32_t)(pid >> 32);
           P.draw = 0;
@@ -813,6 +814,8 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     I.stream = 0;
     (void)stream;
     I.count = pl.nPackets[iL];
+    I.pOff = m->packetOffset;
+    I.pStride = m->packetStride ? m->packetStride : 1;
   }
   return MCB_OK;
 }

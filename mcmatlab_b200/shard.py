@@ -1,0 +1,110 @@
+"""Packet sharding of one MC run over the ranks of a torch.distributed process group.
+
+Packets are independent, so rank r of W runs packets r, r + W, r + 2W, ... of the unsharded
+run's random streams (mcb_mc_model.packetOffset / packetStride) and the normalised outputs are
+merged once at the end with a single all-reduce (NCCL over NVLink on GPUs, gloo on CPUs).
+The merge is the weighted combination MCmatlab itself uses to merge runs
+(+MCmatlab/@model/combineModels.m:59-101): every output of wavelength l is normalised by that
+wavelength's launched packets, so the merged output is sum_r n_{r,l} out_{r,l} / sum_r n_{r,l}.
+For a fixed packet count the shards together launch exactly the packets of the unsharded run,
+so the merged result equals it up to floating-point summation order.
+
+Heat is not sharded: its line solves couple whole grid axes (replicas only).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# outputs merged with per-wavelength weights (last axis = wavelength when nL > 1)
+WEIGHTED = ("NFR", "image", "farField", "NI_xpos", "NI_xneg", "NI_ypos", "NI_yneg", "NI_zpos", "NI_zneg")
+
+
+def shard_count(total, rank, world):
+    """Packets of rank `rank` when `total` packets are dealt round-robin over `world` ranks."""
+    return (int(total) - rank + world - 1) // world if rank < int(total) else 0
+
+
+def wavelength_counts(total, nL):
+    """Packets per wavelength of a fixed-count run (the split of MCmatlab.c:635): an equal
+    share for every wavelength but the last, which takes the remainder."""
+    total = int(total)
+    per = total // nL
+    return [per] * (nL - 1) + [total - per * (nL - 1)]
+
+
+def shard_model(mc_in, rank, world):
+    """The MEX-level inputs of rank `rank`'s shard."""
+    if math.isnan(float(mc_in["nPhotonsRequested"])) or mc_in.get("requestCollectedPhotons"):
+        raise ValueError("sharding needs a fixed launched-packet count")
+    m = dict(mc_in)
+    m["nPhotonsRequested"] = float(shard_count(mc_in["nPhotonsRequested"], rank, world))
+    m["packetOffset"] = int(mc_in.get("packetOffset", 0)) + rank * int(mc_in.get("packetStride", 1))
+    m["packetStride"] = int(mc_in.get("packetStride", 1)) * world
+    if rank != 0:
+        m["nExamplePaths"] = 0
+    return m
+
+
+def _weights(mc_in, rank, world):
+    nL = np.asarray(mc_in["mua"]).shape[1]
+    n_r = wavelength_counts(shard_count(mc_in["nPhotonsRequested"], rank, world), nL)
+    n = wavelength_counts(mc_in["nPhotonsRequested"], nL)
+    return np.array([a / b if b else 0.0 for a, b in zip(n_r, n)]), nL
+
+
+def merge(out, mc_in, rank, world, allreduce):
+    """Combines this rank's outputs with the other ranks' through `allreduce(flat float64 array)
+    -> summed array` (one call). Returns the merged output dict (on every rank)."""
+    w, nL = _weights(mc_in, rank, world)
+    keys, parts, shapes = [], [], []
+    for k in WEIGHTED:
+        a = out.get(k)
+        if a is None or np.size(a) <= 1 or not np.all(np.isfinite(a)):
+            continue
+        a = np.asarray(a, dtype=np.float64)
+        assert a.shape[-1] == nL, k  # every tallied output carries the wavelength as its last axis
+        scaled = a * w
+        keys.append(k)
+        shapes.append(a.shape)
+        parts.append(scaled.reshape(-1, order="F"))
+    counts = np.array([float(out["nPhotons"]), float(out["nPhotonsCollected"]), float(out["nThreads"])])
+    flat = np.concatenate(parts + [counts]) if parts else counts
+    total = allreduce(flat)
+    res = dict(out)
+    off = 0
+    for k, shp in zip(keys, shapes):
+        n = int(np.prod(shp))
+        res[k] = total[off:off + n].reshape(shp, order="F").astype(np.asarray(out[k]).dtype)
+        off += n
+    res["nPhotons"] = total[off]
+    res["nPhotonsCollected"] = total[off + 1]
+    res["nThreads"] = total[off + 2]
+    return res
+
+
+def torch_allreduce(group=None):
+    """all-reduce (sum) of a float64 numpy array through torch.distributed: on the rank's GPU for
+    NCCL, on the host for gloo."""
+    import torch
+    import torch.distributed as dist
+
+    def f(a):
+        dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+        t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t.cpu().numpy()
+    return f
+
+
+def sharded_mc_run(mc_in, run=None, group=None):
+    """runMonteCarlo's MEX call on every rank of `group`: each rank runs its shard with `run`
+    (default: the CUDA transport, native.mc_run) and all ranks return the merged outputs."""
+    import torch.distributed as dist
+    if run is None:
+        from . import native
+        run = native.mc_run
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    out = run(shard_model(mc_in, rank, world))
+    return merge(out, mc_in, rank, world, torch_allreduce(group))

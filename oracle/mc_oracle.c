@@ -84,6 +84,8 @@ typedef struct {
   int aborting;
   /* perturbation MC (gradient runs) */
   int grad, nGM, nR;
+  /* sharding: packet k of this run uses the stream of packet pOff + k * pStride */
+  uint64_t pOff, pStride;
   double rbin;
   int box[6];
   double *gR, *gF;
@@ -802,6 +804,8 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
   R.minIdx = infcast(in->DC_minSubmediaIdx) - 1; R.maxIdx = infcast(in->DC_maxSubmediaIdx) - 1;
   R.onlyCollected = in->DC_onlyCollected;
   R.eol = in->DC_evaluateOnlyAtEndOfLife;
+  R.pOff = in->packetOffset;
+  R.pStride = in->packetStride ? in->packetStride : 1;
   if (R.minS == 0 && R.maxS == ULONG_MAX && R.minRefr == 0 && R.maxRefr == ULONG_MAX && R.minRefl == 0 &&
       R.maxRefl == ULONG_MAX && R.minI == 0 && R.maxI == ULONG_MAX && !R.onlyCollected)
     R.eol = false;
@@ -868,7 +872,7 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
 #pragma omp atomic read
           col = R.nPhotonsCollected;
           if (col >= nReq || R.aborting) break;
-          run_packet(&R, &P, pid);
+          run_packet(&R, &P, R.pOff + R.pStride * pid);
         }
 #pragma omp atomic
         steps += P.steps;
@@ -883,7 +887,7 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
 #pragma omp for schedule(dynamic, 64)
         for (long long pid = 0; pid < (long long)nReq; pid++) {
           if (R.aborting) continue;
-          run_packet(&R, &P, (uint64_t)pid);
+          run_packet(&R, &P, R.pOff + R.pStride * (uint64_t)pid);
         }
 #pragma omp atomic
         steps += P.steps;

@@ -1,0 +1,79 @@
+"""MC packet sharding over a process group: shard arithmetic, and on two gloo ranks (CPU, the
+oracle as each rank's transport) the merged result equals the unsharded run of the same seed."""
+import os
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import mccases
+from mcmatlab_b200 import mexargs, shard
+
+
+def test_shard_counts_partition_packets():
+    for total in (0, 1, 7, 1000, 1001):
+        for world in (1, 2, 3, 8):
+            counts = [shard.shard_count(total, r, world) for r in range(world)]
+            assert sum(counts) == total
+            ids = sorted(r + world * k for r in range(world) for k in range(counts[r]))
+            assert ids == list(range(total))
+    assert shard.wavelength_counts(10, 3) == [3, 3, 4]
+
+
+def _case():
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    mc_in["nPhotonsRequested"] = 4001.0
+    mc_in["seed"] = 5
+    return mc_in
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import orc
+        out = shard.sharded_mc_run(_case(), run=lambda m: orc.oracle_mc(m, 2))
+        if rank == 0:
+            q.put({k: out[k] for k in ("NFR", "NI_zneg", "nPhotons")})
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_merge_to_the_unsharded_run(oracle_lib):
+    from oracle import orc
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    full = orc.oracle_mc(_case(), 4)
+    assert got["nPhotons"] == full["nPhotons"] == 4001
+    for k in ("NFR", "NI_zneg"):
+        a, b = np.asarray(got[k], np.float64), np.asarray(full[k], np.float64)
+        assert np.max(np.abs(a - b)) <= 1e-5 * np.max(np.abs(b)), k
+
+
+def test_shards_run_disjoint_streams(oracle_lib):
+    """Two shards of one seed differ from each other, and the unsharded run is their merge."""
+    from oracle import orc
+    mc_in = _case()
+    outs = [orc.oracle_mc(shard.shard_model(mc_in, r, 2), 2) for r in range(2)]
+    assert not np.allclose(outs[0]["NFR"], outs[1]["NFR"])
+    merged = [None]
+
+    def fake_allreduce(rank):
+        def f(a):
+            merged[0] = a if merged[0] is None else merged[0] + a
+            return merged[0]
+        return f
+    shard.merge(outs[0], mc_in, 0, 2, fake_allreduce(0))
+    res = shard.merge(outs[1], mc_in, 1, 2, fake_allreduce(1))
+    full = orc.oracle_mc(mc_in, 4)
+    assert np.max(np.abs(res["NFR"] - full["NFR"])) <= 1e-5 * np.max(full["NFR"])
