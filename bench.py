@@ -10,7 +10,11 @@ Workload ("coupled heat on config-0 geometry"):
   * one bench step = one call of the stepper over `--nt` DG-ADI time steps with the light on
     (the illumination phase of the schedule; a full update call of that phase is ~1.45e5 steps).
 Metric: heat voxel-updates/s (voxels x time steps / s), whole job. The MC transport of the
-same cube (photon packets/s) is reported in the same line under "mc".
+same cube (photon packets/s) is reported in the same line under "mc" (with N GPUs: N x 1e6
+packets sharded over the ranks, tallies merged by one NCCL all-reduce). On 1 GPU the line also
+carries the batched sweep ("mc_batched": batched launch vs per-instance launches), the
+perturbation-MC gradients ("mc_grad": gradient run vs plain forward on the 256^3 8-medium cube)
+and the heat adjoint ("heat_adjoint": adjoint vs forward on 300x300x200, 2000 steps).
 
 Timing: `value` = device time (CUDA events recorded by the library on its own stream) of the
 stepping loop with all grids resident in HBM; L2 is flushed (256 MB write) between timed steps
@@ -131,17 +135,34 @@ def run_ours(args):
     from mcmatlab_b200 import native
     rank, ws, dist = dist_init()
     dev = torch.cuda.current_device() if torch.cuda.is_available() else 0
-    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=MC_PACKETS, seed=1 + rank)
+    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=MC_PACKETS * ws, seed=1)
     mc_in = mexargs.prepare_mc(m)
-    # warm the transport once, then time it (packets/s on the cube)
+    # warm the transport once, then time it (packets/s on the cube). With N ranks the N x 1e6
+    # packets of one seed are sharded over the ranks (packet r, r + N, ...) and the tallies are
+    # merged by one all-reduce (NCCL); the time is the max over ranks of transport + merge.
     mc_small = dict(mc_in)
     mc_small["nPhotonsRequested"] = 1e5
     native.mc_run(mc_small, device=dev)
+    if dist:
+        from mcmatlab_b200 import shard
+        dist.barrier()
     t0 = time.perf_counter()
-    out = native.mc_run(mc_in, device=dev)
-    mc_wall = time.perf_counter() - t0
-    mc_ms = out["kernelMs"]
-    steps_mc = out["propagationSteps"]
+    if dist:
+        out = native.mc_run(shard.shard_model(mc_in, rank, ws), device=dev)
+        mc_ms = out["kernelMs"]
+        steps_mc = out["propagationSteps"]
+        tm = time.perf_counter()
+        out = shard.merge(out, mc_in, rank, ws, shard.torch_allreduce())
+        merge_ms = (time.perf_counter() - tm) * 1e3
+        t = torch.tensor([mc_ms + merge_ms, time.perf_counter() - t0, float(steps_mc)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[2:], op=dist.ReduceOp.SUM)
+        mc_ms, mc_wall, steps_mc = float(t[0]), float(t[1]), int(t[2])
+    else:
+        out = native.mc_run(mc_in, device=dev)
+        mc_wall = time.perf_counter() - t0
+        mc_ms = out["kernelMs"]
+        steps_mc = out["propagationSteps"]
     NFR = out["NFR"][..., 0]
     mua = mc_in["mua"][:, 0]
     NA = mua[mc_in["M"].astype(np.int64) - 1].astype(np.float32) * NFR
@@ -215,13 +236,19 @@ def run_ours(args):
                      "kernel": "DG-ADI step (pass_x + pass_yz<y> + pass_yz<z>)"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
-        "mc": {"metric": "photon packets/s", "workload": "standard-tissue cube 100^3, pencil beam, 1e6 packets",
-               "value": MC_PACKETS / (mc_ms / 1e3), "e2e_value": MC_PACKETS / mc_wall,
+        "mc": {"metric": "photon packets/s", "workload": "standard-tissue cube 100^3, pencil beam, %d x 1e6 packets" % ws,
+               "value": MC_PACKETS * ws / (mc_ms / 1e3), "e2e_value": MC_PACKETS * ws / mc_wall,
                "kernel_ms": mc_ms, "propagation_steps": steps_mc,
-               "steps_per_s": steps_mc / (mc_ms / 1e3)},
+               "steps_per_s": steps_mc / (mc_ms / 1e3),
+               "parallelism": "packets sharded over %d ranks, one NCCL all-reduce of the tallies" % ws if ws > 1 else "1 GPU"},
     }
-    if args.c2:
+    # the remaining measurements are single-GPU ones (run on 1-GPU invocations only)
+    if args.c2 and ws == 1:
         res["mc_batched"] = batched_sweep_measure(dev, args.c2_instances, args.c2_scale)
+    if args.c3 and ws == 1:
+        res["mc_grad"] = grad_measure(dev, args.c3_packets, args.c3_grid)
+    if args.c4 and ws == 1:
+        res["heat_adjoint"] = adjoint_measure(dev, args.c4_steps)
     if rank == 0:
         if args.cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
@@ -259,6 +286,45 @@ def batched_sweep_measure(dev, n_inst, scale):
             "ratio_device": plain_ms / batch_ms,
             "batched_e2e_packets_per_s": total / batch_wall, "plain_e2e_packets_per_s": total / plain_wall,
             "ratio_e2e": plain_wall / batch_wall}
+
+
+def grad_measure(dev, packets, n):
+    """Perturbation-MC gradients on the 0.5 cm, 8-medium cube (n^3 voxels): 32 radial reflectance
+    bins and the mean fluence of a 16^3 box, d/dmua and d/dmus of every medium, against one plain
+    forward run of the same packets."""
+    from mcmatlab_b200 import native
+    mc_in = mexargs.prepare_mc(configs.perturbation_cube(n=n, nPhotons=packets))
+    z0 = n // 6
+    box = [n // 2 - 8, n // 2 + 8, n // 2 - 8, n // 2 + 8, z0, z0 + 16]
+    obj = dict(nRadialBins=32, radialBinWidth=0.25 / 32, box=box)
+    native.mc_run(dict(mc_in, nPhotonsRequested=1e5), device=dev)
+    native.mc_grad(dict(mc_in, nPhotonsRequested=1e5), device=dev, **obj)
+    fwd = native.mc_run(mc_in, device=dev)
+    o, g = native.mc_grad(mc_in, device=dev, **obj)
+    return {"workload": "perturbation MC, %d^3 voxels over a 0.5 cm cube, 8 tissue media + air, %.0e packets, "
+                        "32 radial reflectance bins + 16^3-box fluence, d/dmua and d/dmus of 9 media" % (n, packets),
+            "forward_packets_per_s": packets / (fwd["kernelMs"] / 1e3),
+            "grad_packets_per_s": packets / (o["kernelMs"] / 1e3),
+            "forward_ms": fwd["kernelMs"], "grad_ms": o["kernelMs"],
+            "grad_over_forward": o["kernelMs"] / fwd["kernelMs"], "target_grad_over_forward": 1.5}
+
+
+def adjoint_measure(dev, nt):
+    """Heat adjoint on 300x300x200 voxels (4 seeded media, Gaussian source, damage and peak
+    objectives) with ceil(sqrt(nt)) checkpoints, against the plain forward of the same steps."""
+    from mcmatlab_b200 import native
+    case = configs.heat_adjoint_case(nt=nt)
+    nx, ny, nz = case["n"]
+    native.heat_forward(case["T0"], None, dict(case["hp"], steps=4.0), nx, ny, nz, device=dev)
+    native.heat_forward(case["T0"], None, case["hp"], nx, ny, nz, device=dev)
+    fwd_ms = native.last_kernel_ms(dev)
+    g = native.heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"], device=dev)
+    L = nx * ny * nz
+    return {"workload": "heat adjoint, 300x300x200 voxels, 4 media, %d steps, %d checkpoints, damage + peak objectives"
+                        % (nt, math.ceil(math.sqrt(nt))),
+            "forward_voxel_updates_per_s": L * nt / (fwd_ms / 1e3), "forward_ms": fwd_ms,
+            "adjoint_forward_sweep_ms": g["forwardMs"], "adjoint_reverse_sweep_ms": g["adjointMs"],
+            "adjoint_over_forward": (g["forwardMs"] + g["adjointMs"]) / fwd_ms}
 
 
 def reference_setup():
@@ -339,6 +405,11 @@ def main():
     ap.add_argument("--no-c2", dest="c2", action="store_false", help="skip the batched-sweep measurement")
     ap.add_argument("--c2-instances", type=int, default=64)
     ap.add_argument("--c2-scale", type=float, default=1.0, help="photon-count scale of the batched sweep")
+    ap.add_argument("--no-c3", dest="c3", action="store_false", help="skip the perturbation-MC gradient measurement")
+    ap.add_argument("--c3-packets", type=float, default=1e8)
+    ap.add_argument("--c3-grid", type=int, default=256)
+    ap.add_argument("--no-c4", dest="c4", action="store_false", help="skip the heat-adjoint measurement")
+    ap.add_argument("--c4-steps", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
