@@ -72,7 +72,6 @@ struct Inst {
 
 constexpr int kGradMedia = 10;  // media supported by gradient runs
 
-// Per-packet perturbation-MC state: path length L_m and scattering count k_m per medium.
 // d/dmua of c(mua) = w (1 - exp(-mua s)) / mua is w s^2 phi(mua s) with
 // phi(x) = (exp(-x) - (1 - exp(-x)) / x) / x; its Taylor series -1/2 + x/3 - x^2/8 + x^3/30
 // replaces the cancelling direct form for small x (air has mua = 1e-8 /cm)
@@ -80,11 +79,6 @@ __device__ __forceinline__ float self_phi(float x) {
   if (x < 0.05f) return -0.5f + x * (1.f / 3.f - x * (0.125f - x * (1.f / 30.f)));
   return (expf(-x) + expm1f(-x) / x) / x;
 }
-
-struct GradState {
-  float L[kGradMedia];
-  float k[kGradMedia];
-};
 
 struct Photon {
   float i[3], u[3], D[3];

@@ -94,17 +94,18 @@ __device__ __forceinline__ unsigned long long fetch_packet(const KernelArgs &a) 
 }
 
 
-// Launch bounds: the plain kernel fits 3 blocks of 256 per SM without spills; the gradient
-// variant carries per-packet path lengths, scattering counts and box partial sums (2 blocks).
+// Launch bounds: 3 blocks of 256 per SM without spills. The gradient variant keeps its
+// per-packet state (path length L_m and scattering count k_m per medium) and its per-thread box
+// partial sums in dynamic shared memory, one column per thread (grad_smem_bytes), so that it
+// runs at the plain kernel's occupancy; the medium index selects the row directly.
 template <bool GRAD>
-__global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
   // single-instance runs read the instance and its medium table from shared memory
   __shared__ Inst sInst;
   __shared__ float4 sMed[256];
   __shared__ int sCdf[256];
-  __shared__ double sR[GRAD ? 64 * (1 + 2 * kGradMedia) : 1];
-  __shared__ double sF[GRAD ? 1 + 2 * kGradMedia : 1];
   __shared__ float sInvMus[kGradMedia];
+  extern __shared__ double gradSmem[];
   const bool single = a.nInst == 1;
   if (single) {
     const Inst *g0 = a.insts;
@@ -121,23 +122,28 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
     __syncthreads();
   }
   int nGM = 0, nGR = 0;
+  // gradient state (GRAD only): radial-bin and box sums of the block, and per-thread columns
+  // (stride blockDim.x) of L_m, k_m and the thread's box partial sums [value, d/dmua, d/dmus]
+  double *sR = gradSmem, *sF = gradSmem;
+  float *sGL = nullptr, *sGK = nullptr, *sBox = nullptr;
+  const int tid = threadIdx.x, bd = blockDim.x;
   if (GRAD) {
     // gradient runs are single-instance (enforced by the host)
     nGM = sInst.nM;
     nGR = sInst.nR;
+    sF = sR + nGR * (1 + 2 * nGM);
+    sGL = (float *)(sF + 1 + 2 * nGM);
+    sGK = sGL + nGM * bd;
+    sBox = sGK + nGM * bd;
     for (int k = threadIdx.x; k < nGR * (1 + 2 * nGM); k += blockDim.x) sR[k] = 0.0;
     for (int k = threadIdx.x; k < 1 + 2 * nGM; k += blockDim.x) sF[k] = 0.0;
     for (int k = threadIdx.x; k < nGM; k += blockDim.x) sInvMus[k] = 1.0f / sMed[k].y;
+    for (int q = 0; q < 1 + 2 * nGM; q++) sBox[q * bd + tid] = 0.f;
     __syncthreads();
   }
   Photon P;
   P.alive = false;
   P.inbox = false;
-  GradState Gs;
-  // per-thread partial sums of the box objective and its derivatives (flushed once at exit)
-  float boxAcc[GRAD ? 1 + 2 * kGradMedia : 1];
-#pragma unroll
-  for (int q = 0; q < (GRAD ? 1 + 2 * kGradMedia : 1); q++) boxAcc[q] = 0.f;
   const Inst *I = single ? &sInst : a.insts;
   bool replay = false;
   bool started = false;
@@ -190,10 +196,9 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
             atomicAdd(&I->ctr[0], 1ull);
             started = true;
             if (GRAD) {
-#pragma unroll
-              for (int m = 0; m < kGradMedia; m++) {
-                Gs.L[m] = 0.f;
-                Gs.k[m] = 0.f;
+              for (int m = 0; m < nGM; m++) {
+                sGL[m * bd + tid] = 0.f;
+                sGK[m * bd + tid] = 0.f;
               }
               P.inbox = in_box(*I, P.i);
             }
@@ -224,19 +229,16 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
             const float c = absorb / mua;
             const float dself = wpre * s * s * self_phi(mua * s);
             const float kself = P.stepLeft > 0 ? 0.f : 1.f;
-            boxAcc[0] += c;
-#pragma unroll
-            for (int m = 0; m < kGradMedia; m++) {
-              if (m < nGM) {
-                const float Lincl = Gs.L[m] + (m == mj ? s : 0.f);
-                const float kincl = Gs.k[m] + (m == mj ? kself : 0.f);
-                boxAcc[1 + m] += -Gs.L[m] * c + (m == mj ? dself : 0.f);
-                boxAcc[1 + kGradMedia + m] += (kincl * sInvMus[m] - Lincl) * c;
-              }
+            sBox[tid] += c;
+            for (int m = 0; m < nGM; m++) {
+              const float Lm = sGL[m * bd + tid];
+              const float Lincl = Lm + (m == mj ? s : 0.f);
+              const float kincl = sGK[m * bd + tid] + (m == mj ? kself : 0.f);
+              sBox[(1 + m) * bd + tid] += -Lm * c + (m == mj ? dself : 0.f);
+              sBox[(1 + nGM + m) * bd + tid] += (kincl * sInvMus[m] - Lincl) * c;
             }
           }
-#pragma unroll
-          for (int m = 0; m < kGradMedia; m++) Gs.L[m] += (m == mj ? s : 0.f);
+          sGL[mj * bd + tid] += s;
         }
         if (P.inside && I->NFR) {
           double c = 0.0;
@@ -269,12 +271,10 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
               const float W = P.weight;
               double *row = sR + b * (1 + 2 * nGM);
               atomicAdd(row, (double)W);
-#pragma unroll
-              for (int m = 0; m < kGradMedia; m++) {
-                if (m < nGM) {
-                  atomicAdd(row + 1 + m, (double)(-Gs.L[m] * W));
-                  atomicAdd(row + 1 + nGM + m, (double)((Gs.k[m] * sInvMus[m] - Gs.L[m]) * W));
-                }
+              for (int m = 0; m < nGM; m++) {
+                const float Lm = sGL[m * bd + tid];
+                atomicAdd(row + 1 + m, (double)(-Lm * W));
+                atomicAdd(row + 1 + nGM + m, (double)((sGK[m * bd + tid] * sInvMus[m] - Lm) * W));
               }
             }
           }
@@ -290,11 +290,7 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
           else P.alive = false;
         }
         if (P.alive) {
-          if (GRAD) {
-            const int mj = P.med;
-#pragma unroll
-            for (int m = 0; m < kGradMedia; m++) Gs.k[m] += (m == mj ? 1.f : 0.f);
-          }
+          if (GRAD) sGK[P.med * bd + tid] += 1.f;
           scatter(P, *I);
         }
       }
@@ -303,16 +299,8 @@ __global__ void __launch_bounds__(256, GRAD ? 2 : 3) transport_kernel(KernelArgs
   // lanes leave the loop at different times, so each adds its own count
   atomicAdd(a.steps, steps);
   if (GRAD) {
-    if (nGM > 0 && (I->box[1] > I->box[0])) {
-      atomicAdd(&sF[0], (double)boxAcc[0]);
-#pragma unroll
-      for (int m = 0; m < kGradMedia; m++) {
-        if (m < nGM) {
-          atomicAdd(&sF[1 + m], (double)boxAcc[1 + m]);
-          atomicAdd(&sF[1 + nGM + m], (double)boxAcc[1 + kGradMedia + m]);
-        }
-      }
-    }
+    if (nGM > 0 && (I->box[1] > I->box[0]))
+      for (int q = 0; q < 1 + 2 * nGM; q++) atomicAdd(&sF[q], (double)sBox[q * bd + tid]);
     __syncthreads();
     for (int k = threadIdx.x; k < nGR * (1 + 2 * nGM); k += blockDim.x)
       if (sR[k] != 0.0) atomicAdd(&sInst.gR[k], sR[k]);
@@ -820,6 +808,12 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
   return MCB_OK;
 }
 
+// Dynamic shared memory of the gradient kernel: the block's radial-bin and box sums (FP64) and
+// per-thread columns of L_m, k_m and the box partial sums (FP32).
+size_t grad_smem_bytes(int nM, int nR, int threads) {
+  return 8 * (size_t)(nR * (1 + 2 * nM) + 1 + 2 * nM) + 4 * (size_t)threads * (2 * nM + 1 + 2 * nM);
+}
+
 mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &insts, bool openEnded,
                             unsigned long long collectTarget, double seconds, unsigned long long *stepsOut,
                             float *msOut, int *statusOut, bool grad = false) {
@@ -850,8 +844,11 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
   a.deadlineNs = 0;
   a.refillMin = 8;
   if (const char *e = std::getenv("MCB_REFILL_MIN")) a.refillMin = std::max(1, std::min(32, std::atoi(e)));
+  const size_t dynSmem = grad ? grad_smem_bytes(insts[0].nM, insts[0].nR, 256) : 0;
+  if (grad)
+    MCB_CUDA(ctx, cudaFuncSetAttribute(transport_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynSmem));
   int blocksPerSm = 0;
-  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, grad ? transport_kernel<true> : transport_kernel<false>, 256, 0));
+  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, grad ? transport_kernel<true> : transport_kernel<false>, 256, dynSmem));
   if (blocksPerSm < 1) blocksPerSm = 1;
   const int grid = ctx->num_sms * blocksPerSm;
   if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
@@ -865,7 +862,7 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
     a.deadlineNs = now + (unsigned long long)(seconds * 1e9);
   }
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-  if (grad) transport_kernel<true><<<grid, 256, 0, st>>>(a);
+  if (grad) transport_kernel<true><<<grid, 256, dynSmem, st>>>(a);
   else transport_kernel<false><<<grid, 256, 0, st>>>(a);
   MCB_CUDA(ctx, cudaGetLastError());
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
