@@ -236,7 +236,7 @@ MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, cons
  * a PyTorch caching allocator, has already reserved; other streams' work that cudaFree's
  * device-wide synchronisation would stall). Same arguments, outputs and errors as
  * mcb_heat_forward. Its working set lives in one static 32 MiB device array of the library:
- * 37 bytes per voxel (29 without damage, 33 with damage but no light) plus 8 per sensor and
+ * 66 bytes per voxel (58 without damage, 62 with damage but no light) plus 8 per sensor and
  * step (sensorTemps history) and small per-medium tables; larger problems return MCB_EINVAL
  * naming the limit. The context comes from mcb_ctx_create, which does allocate: create it
  * at set-up. The first call on a device performs set-up (cudaGetSymbolAddress of the scratch);

@@ -2,15 +2,16 @@
 // (replacing +MCmatlab/src/finiteElementHeatPropagator.c:688-821).
 //
 // One time step of the reference is six grid passes (substep1a..3b, :249-647). Here it is
-// three, one per direction, each fusing the explicit half with the implicit line solve:
-//   X pass: rhs = T + dt(Q + x/2 + y + z) on T^n (1a), tridiagonal solve along x (1b) -> A
-//   Y pass: rhs = A - dt/2 y(T^n) (2a), solve along y (2b)                             -> A
-//   Z pass: rhs = A - dt/2 z(T^n) (3a), solve along z (3b), Arrhenius damage with the
-//           mid-step temperature and per-medium running maxima                          -> T
-// The tridiagonal matrices depend only on (M, c, dt, boundary type), so their pivots are
-// factored once per call (inverse pivots per voxel and direction); each pass then solves its
-// lines with a warp-parallel chunked scan of the two first-order recurrences of the Thomas
-// algorithm instead of one serial thread per line.
+// three, one per direction. All explicit work happens in the first, which reads T^n once:
+//   X pass: rhs = T + dt(Q + x/2 + y + z) on T^n (1a), solve along x (1b); it also forms the
+//           half-corrections S_y = dt/2 y(T^n), S_z = dt/2 z(T^n) of 2a and 3a  -> A1 - S_y, S_z
+//   Y pass: solve along y (2b) on A1 - S_y                                       -> A2
+//   Z pass: solve along z (3b) on A2 - S_z, Arrhenius damage with the mid-step
+//           temperature and per-medium running maxima                             -> T
+// The tridiagonal matrices depend only on (M, c, dt, boundary type), so each voxel's inverse
+// pivot and scan multipliers are factored once per call; each pass then solves its lines with
+// a warp-parallel chunked scan of the two first-order recurrences of the Thomas algorithm
+// instead of one serial thread per line.
 //
 // Temperatures are stored as deviations from a per-call base temperature (the mean input
 // temperature). The scheme is linear and shift-invariant in T, so this is exact algebra; it
@@ -44,8 +45,9 @@ __device__ void record_sensors(const HeatDev &h, int col) {
 }
 
 
-// Inverse pivots 1/b'_i of each line's matrix, one thread per line (once per call and dt).
-__global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
+// Line factorisation, once per call and dt: inverse pivots 1/b'_i and the two scan multipliers
+// {fm_i, bm_i} = {a_i / b'_{i-1}, cc_i / b'_i} of every voxel's row, one thread per line.
+__global__ void factor_kernel(HeatDev h, int dir, float *ibOut, float2 *fbOut) {
   const int nx = h.nx, ny = h.ny, nz = h.nz;
   const long long nLines = dir == 0 ? (long long)ny * nz : (dir == 1 ? (long long)nx * nz : (long long)nx * ny);
   const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
@@ -59,7 +61,7 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
     const bool lineSinked = h.hs && (dir == 0 ? (iy0 == 0 || iy0 == ny - 1 || iz0 == 0 || iz0 == nz - 1)
                                      : dir == 1 ? (ix0 == 0 || ix0 == nx - 1 || iz0 == 0 || iz0 == nz - 1)
                                                 : (ix0 == 0 || ix0 == nx - 1 || iy0 == 0 || iy0 == ny - 1));
-    float bprev = 1.f, ccprev = 0.f;
+    float bprev = 1.f, ccprev = 0.f, ibprev = 1.f;
     for (int i = 0; i < n; i++) {
       const long long v = base + i * st;
       float a = 0.f, cc = 0.f;
@@ -70,18 +72,95 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut) {
       }
       float b = 1.f + a + cc;
       if (i > 0) b -= a * ccprev / bprev;
-      ibOut[v] = 1.f / b;
+      const float ib = 1.f / b;
+      ibOut[v] = ib;
+      fbOut[v] = make_float2(i > 0 ? a * ibprev : 0.f, cc * ib);
       bprev = b;
       ccprev = cc;
+      ibprev = ib;
     }
   }
 }
 
-// X pass: explicit 1a + solve along x. A block owns h.xl consecutive x-lines (consecutive y at
-// one z); each line's rhs, multipliers and pivots are formed in shared memory, then the lines
-// are solved together.
+// Neighbourhood code of every voxel (once per call): bit 2d (2d+1) is set when the lower
+// (upper) neighbour along d is missing or of another medium; kNbSink marks heat-sinked voxels.
+constexpr int kNbSink = 64;
+__global__ void neighbour_code_kernel(HeatDev h, uint8_t *out) {
+  const long long sxy = (long long)h.nx * h.ny, L = sxy * h.nz;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(v / sxy);
+    const long long r = v - iz * sxy;
+    const int iy = (int)(r / h.nx), ix = (int)(r - (long long)iy * h.nx);
+    const int m = h.M[v];
+    int code = sinked(h, ix, iy, iz) ? kNbSink : 0;
+    if (ix == 0 || h.M[v - 1] != m) code |= 1;
+    if (ix == h.nx - 1 || h.M[v + 1] != m) code |= 2;
+    if (iy == 0 || h.M[v - h.nx] != m) code |= 4;
+    if (iy == h.ny - 1 || h.M[v + h.nx] != m) code |= 8;
+    if (iz == 0 || h.M[v - sxy] != m) code |= 16;
+    if (iz == h.nz - 1 || h.M[v + sxy] != m) code |= 32;
+    out[v] = (uint8_t)code;
+  }
+}
 
-__global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
+// Loads of one voxel's explicit stencil (T^n and its six neighbours, code, medium, source) and
+// the stencil itself: rhs1 = T + dt (Q + D_y T + D_z T) + dt/2 D_x T, with the half-corrections
+// S_y = dt/2 D_y T and S_z = dt/2 D_z T that the Y and Z solves subtract. Voxels whose six
+// neighbours exist and share their medium (neighbourhood code 0) take the diagonal coefficients
+// c(m, m, d); the others look every face up. Heat-sinked voxels keep T (identity rows).
+struct VoxIn {
+  float t, n[6], q;
+  int code, m;
+};
+
+__device__ __forceinline__ void voxel_load(const HeatDev &h, int v, int x, int iy, int iz, VoxIn &o) {
+  const int nx = h.nx, ny = h.ny, nz = h.nz, sxy = nx * ny;
+  const float *__restrict__ T = h.T;
+  o.code = h.nb[v];
+  o.t = T[v];
+  o.m = h.M[v];
+  o.q = h.Q ? h.Q[v] : 0.f;
+  o.n[0] = x > 0 ? T[v - 1] : 0.f;
+  o.n[1] = x < nx - 1 ? T[v + 1] : 0.f;
+  o.n[2] = iy > 0 ? T[v - nx] : 0.f;
+  o.n[3] = iy < ny - 1 ? T[v + nx] : 0.f;
+  o.n[4] = iz > 0 ? T[v - sxy] : 0.f;
+  o.n[5] = iz < nz - 1 ? T[v + sxy] : 0.f;
+}
+
+__device__ __forceinline__ void voxel_explicit(const HeatDev &h, int v, int x, int iy, int iz, const VoxIn &a, float &r,
+                                               float &hy, float &hz) {
+  const int nx = h.nx, ny = h.ny, nz = h.nz, sxy = nx * ny;
+  const float t = a.t;
+  r = t;
+  hy = hz = 0.f;
+  if (a.code & kNbSink) return;
+  const int mi = a.m;
+  float dx, dy, dz;
+  if ((a.code & 63) == 0) {
+    dx = cf(h, mi, mi, 0) * (a.n[0] + a.n[1] - 2.f * t);
+    dy = cf(h, mi, mi, 1) * (a.n[2] + a.n[3] - 2.f * t);
+    dz = cf(h, mi, mi, 2) * (a.n[4] + a.n[5] - 2.f * t);
+  } else {
+    dx = dy = dz = 0.f;
+    if (x > 0) dx += cf(h, mi, h.M[v - 1], 0) * (a.n[0] - t);
+    if (x < nx - 1) dx += cf(h, mi, h.M[v + 1], 0) * (a.n[1] - t);
+    if (iy > 0) dy += cf(h, mi, h.M[v - nx], 1) * (a.n[2] - t);
+    if (iy < ny - 1) dy += cf(h, mi, h.M[v + nx], 1) * (a.n[3] - t);
+    if (iz > 0) dz += cf(h, mi, h.M[v - sxy], 2) * (a.n[4] - t);
+    if (iz < nz - 1) dz += cf(h, mi, h.M[v + sxy], 2) * (a.n[5] - t);
+  }
+  r = t + h.dt * (a.q + dy + dz) + h.hdt * dx;
+  hy = h.hdt * dy;
+  hz = h.hdt * dz;
+}
+
+// X pass: the whole explicit stencil of the step (1a, 2a, 3a) and the solve along x (1b).
+// A block owns h.xl consecutive x-lines (consecutive y at one z); U elements per thread are
+// loaded at a time (all their global loads issued before use). S_y is subtracted from the x
+// solution here, which gives the Y pass its right-hand side A1 - S_y; S_z is stored for the
+// Z pass.
+__global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
   const int nx = h.nx, ny = h.ny, nz = h.nz;
   const int sxy = nx * ny;
@@ -91,8 +170,10 @@ __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
   float *fm = rhs + XL * P;
   float *bm = fm + XL * P;
   float *ib = bm + XL * P;
+  float *sy = ib + XL * P;
   if (blockIdx.x == 0 && h.nS > 0) record_sensors(h, *h.stepCounter);
   const float *ibx = h.ib;
+  const float2 *fbx = h.fb;
   const int yTiles = (ny + XL - 1) / XL;
   for (int tile = blockIdx.x; tile < yTiles * nz; tile += gridDim.x) {
     const int y0 = (tile % yTiles) * XL, iz = tile / yTiles;
@@ -100,36 +181,18 @@ __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
     const int total = cnt * nx;
     constexpr int U = 4;
     for (int e0 = threadIdx.x; e0 < total; e0 += blockDim.x * U) {
-      float vr[U], vf[U], vb[U], vi[U];
+      VoxIn in[U];
+      float vi[U];
+      float2 vf[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int e = e0 + u * blockDim.x;
-        vr[u] = vf[u] = vb[u] = vi[u] = 0.f;
         if (e < total) {
           const int l = e / nx, x = e - l * nx;
-          const int iy = y0 + l;
-          const int v = x + iy * nx + iz * sxy;
-          const bool lineSinked = h.hs && (iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1);
-          const int mi = h.M[v];
-          const float ibv = ibx[v];
-          const float t = h.T[v];
-          float r = t, a = 0.f, cc = 0.f;
-          if (!row_sinked(h, lineSinked, x, nx)) {
-            float syz = 0.f;
-            if (x > 0) a = h.hdt * cf(h, mi, h.M[v - 1], 0);
-            if (x < nx - 1) cc = h.hdt * cf(h, mi, h.M[v + 1], 0);
-            const float sx = (x > 0 ? a * (h.T[v - 1] - t) : 0.f) + (x < nx - 1 ? cc * (h.T[v + 1] - t) : 0.f);
-            if (iy > 0) syz += cf(h, mi, h.M[v - nx], 1) * (h.T[v - nx] - t);
-            if (iy < ny - 1) syz += cf(h, mi, h.M[v + nx], 1) * (h.T[v + nx] - t);
-            if (iz > 0) syz += cf(h, mi, h.M[v - sxy], 2) * (h.T[v - sxy] - t);
-            if (iz < nz - 1) syz += cf(h, mi, h.M[v + sxy], 2) * (h.T[v + sxy] - t);
-            const float q = h.Q ? h.Q[v] : 0.f;
-            r = t + h.dt * (q + syz) + sx;
-          }
-          vr[u] = r;
-          vf[u] = x > 0 ? a * ibx[v - 1] : 0.f;
-          vb[u] = cc * ibv;
-          vi[u] = ibv;
+          const int v = x + (y0 + l) * nx + iz * sxy;
+          voxel_load(h, v, x, y0 + l, iz, in[u]);
+          vi[u] = ibx[v];
+          vf[u] = fbx[v];
         }
       }
 #pragma unroll
@@ -137,10 +200,15 @@ __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
         const int e = e0 + u * blockDim.x;
         if (e < total) {
           const int l = e / nx, x = e - l * nx;
-          rhs[l * P + x] = vr[u];
-          fm[l * P + x] = vf[u];
-          bm[l * P + x] = vb[u];
+          const int v = x + (y0 + l) * nx + iz * sxy;
+          float r, hy, hz;
+          voxel_explicit(h, v, x, y0 + l, iz, in[u], r, hy, hz);
+          h.Sz[v] = hz;
+          rhs[l * P + x] = r;
+          fm[l * P + x] = vf[u].x;
+          bm[l * P + x] = vf[u].y;
           ib[l * P + x] = vi[u];
+          sy[l * P + x] = hy;
         }
       }
     }
@@ -149,7 +217,7 @@ __global__ void __launch_bounds__(256) pass_x_kernel(HeatDev h) {
     __syncthreads();
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int l = e / nx, x = e - l * nx;
-      h.A[x + (y0 + l) * nx + iz * sxy] = rhs[l * P + x];
+      h.A[x + (y0 + l) * nx + iz * sxy] = rhs[l * P + x] - sy[l * P + x];
     }
     __syncthreads();
   }
@@ -161,11 +229,14 @@ __host__ __device__ constexpr size_t yz_tile_bytes(int n) {
 }
 
 // Y and Z passes: a block owns TW consecutive x positions and one line per x along `dir`
-// (dir 1: fixed iz; dir 2: fixed iy). Rows of TW values are read and written coalesced (loads
-// batched per thread for memory-level parallelism); coefficients are formed in parallel, then
-// the TW lines are solved together from shared memory.
+// (dir 1: fixed iz; dir 2: fixed iy). Right-hand sides come from the previous pass (Y: A1 - S_y
+// as the X pass wrote it; Z: A2 - S_z). The tile's rows (TW values each, coalesced) of rhs,
+// pivots, multiplier pairs (and S_z) are staged with asynchronous copies, all in flight at
+// once, then the TW lines are solved together from shared memory. The Z pass adds the
+// Arrhenius damage with the mid-step temperature and the per-medium running maxima, and writes
+// T^{n+1}.
 template <int TW, bool ZPASS>
-__global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
+__global__ void __launch_bounds__(256, 3) pass_yz_kernel(HeatDev h) {
   extern __shared__ unsigned char smem[];
   constexpr int P = TW + 1;  // padded pitch
   const int nx = h.nx, ny = h.ny, nz = h.nz;
@@ -173,16 +244,16 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
   const int n = ZPASS ? nz : ny;
   const int st = ZPASS ? sxy : nx;
   const int dir = ZPASS ? 2 : 1;
-  float *tn = (float *)smem;
-  float *rhs = tn + n * P;
+  float *rhs = (float *)smem;
   float *ib = rhs + n * P;
-  float *fm = ib + n * P;
-  float *bm = fm + n * P;
-  uint8_t *Ms = (uint8_t *)(bm + n * P);
+  float2 *fb = (float2 *)(ib + n * P);
+  float *sz = (float *)(fb + n * P);
+  uint8_t *Ms = (uint8_t *)(sz + n * P);
   __shared__ unsigned int mloc[256];
   const int xTiles = (nx + TW - 1) / TW;
   const int nOther = ZPASS ? ny : nz;
   const float *ibd = h.ib + (size_t)dir * sxy * nz;
+  const float2 *fbd = h.fb + (size_t)dir * sxy * nz;
   if (ZPASS) {
     for (int k = threadIdx.x; k < h.nM; k += blockDim.x) mloc[k] = 0u;
   }
@@ -195,60 +266,38 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
     const int x0 = (tile % xTiles) * TW;
     const int other = tile / xTiles;
     const int base = ZPASS ? other * nx : other * sxy;
-    const bool otherSinked = h.hs && (other == 0 || other == nOther - 1);
     const int x = x0 + cx;
-    // stage T^n, A, M and pivots
-    for (int rb = r0; rb < n; rb += RPI * U) {
-      float vT[U], vA[U], vI[U];
-      uint8_t vM[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int r = rb + u * RPI;
-        if (r < n && x < nx) {
-          const int v = base + x + r * st;
-          vT[u] = h.T[v];
-          vA[u] = h.A[v];
-          vI[u] = ibd[v];
-          vM[u] = h.M[v];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int r = rb + u * RPI;
-        if (r < n && x < nx) {
-          tn[r * P + cx] = vT[u];
-          rhs[r * P + cx] = vA[u];
-          ib[r * P + cx] = vI[u];
-          Ms[r * TW + cx] = vM[u];
-        }
-      }
-    }
-    __syncthreads();
-    // explicit half-correction on T^n (2a / 3a) and the line multipliers
     if (x < nx) {
-      const bool lineSinked = otherSinked || (h.hs && (x == 0 || x == nx - 1));
       for (int r = r0; r < n; r += RPI) {
-        float a = 0.f, cc = 0.f;
-        if (!row_sinked(h, lineSinked, r, n)) {
-          const int mi = Ms[r * TW + cx];
-          const float t = tn[r * P + cx];
-          float sm = 0.f;
-          if (r > 0) {
-            a = h.hdt * cf(h, mi, Ms[(r - 1) * TW + cx], dir);
-            sm += a * (tn[(r - 1) * P + cx] - t);
+        const int v = base + x + r * st;
+        cp_async4(&rhs[r * P + cx], &h.A[v]);
+        cp_async4(&ib[r * P + cx], &ibd[v]);
+        cp_async8(&fb[r * P + cx], &fbd[v]);
+        if (ZPASS) cp_async4(&sz[r * P + cx], &h.Sz[v]);
+      }
+      if (ZPASS) {
+        // media (bytes) for the damage and maxima, U rows in flight per thread
+        for (int rb = r0; rb < n; rb += RPI * U) {
+          uint8_t vM[U];
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            const int r = rb + u * RPI;
+            if (r < n) vM[u] = h.M[base + x + r * st];
           }
-          if (r < n - 1) {
-            cc = h.hdt * cf(h, mi, Ms[(r + 1) * TW + cx], dir);
-            sm += cc * (tn[(r + 1) * P + cx] - t);
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            const int r = rb + u * RPI;
+            if (r < n) Ms[r * TW + cx] = vM[u];
           }
-          rhs[r * P + cx] -= sm;
         }
-        fm[r * P + cx] = r > 0 ? a * ib[(r - 1) * P + cx] : 0.f;
-        bm[r * P + cx] = cc * ib[r * P + cx];
       }
     }
+    cp_async_wait_all();
+    if (ZPASS && x < nx) {
+      for (int r = r0; r < n; r += RPI) rhs[r * P + cx] -= sz[r * P + cx];
+    }
     __syncthreads();
-    solve_lines(rhs, fm, bm, ib, n, P, 1, min(TW, nx - x0));
+    solve_lines(rhs, (const float *)fb, (const float *)fb + 1, ib, n, P, 1, min(TW, nx - x0), 2);
     __syncthreads();
     if (x < nx) {
       for (int r = r0; r < n; r += RPI) {
@@ -259,7 +308,7 @@ __global__ void __launch_bounds__(256) pass_yz_kernel(HeatDev h) {
           if (h.dOmega && h.E[m] != 0.0) {
             // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602),
             // exponent evaluated in FP64 (logA ~ 154 cancels against E/RT)
-            const double tmid = 0.5 * ((double)tnew + (double)tn[r * P + cx]) + h.base + kCelsiusZero;
+            const double tmid = 0.5 * ((double)tnew + (double)h.T[v]) + h.base + kCelsiusZero;
             const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tmid));
             h.dOmega[v] += (float)(h.dtd * rate);
           }
@@ -333,7 +382,7 @@ size_t yz_smem(int TW, int n) {
   return (TW == 32 ? yz_tile_bytes<32>(n) : TW == 16 ? yz_tile_bytes<16>(n) : yz_tile_bytes<8>(n)) + 64;
 }
 
-size_t x_smem_lines(int nx, int xl) { return (size_t)xl * 4 * 4 * (nx + 1) + 64; }
+size_t x_smem_lines(int nx, int xl) { return (size_t)xl * 5 * 4 * (nx + 1) + 64; }
 
 // x-lines per X-pass block: the most that keeps the block's shared memory within 100 KB
 int x_lines(int nx) {
@@ -343,6 +392,7 @@ int x_lines(int nx) {
 }
 
 size_t x_smem(int nx) { return x_smem_lines(nx, x_lines(nx)); }
+
 
 template <int TW>
 mcb_status setup_yz(mcb_ctx *ctx, int ny, int nz) {
@@ -403,8 +453,9 @@ void free_state_buffers(mcb_heat_state *s) {
 mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
   const long long L = (long long)p->nx * p->ny * p->nz;
   const int nM = p->nM;
-  const size_t need = 4 * L * 4 /*T A Q stage*/ + 12 * L + (damage ? 8 * L : 0) + L + 12 * (size_t)nM * nM + 16 * (size_t)nM +
-                      4 * (size_t)nM + 64 + 20 * 256;
+  const size_t need = 4 * L * 3 /*T A Q*/ + 4 * (size_t)std::max<long long>(L, nM) /*stage*/ + 12 * L /*ib*/ +
+                      24 * L /*fb*/ + L /*nb*/ + 4 * L /*Sz*/ + (damage ? 8 * L : 0) + L + 12 * (size_t)nM * nM +
+                      16 * (size_t)nM + 4 * (size_t)nM + 64 + 24 * 256;
   free_state_buffers(s);
   MCB_CUDA(ctx, cudaMalloc(&s->block, need));
   char *cur = (char *)s->block;
@@ -416,8 +467,11 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   s->T = (float *)take(4 * L);
   s->A = (float *)take(4 * L);
   s->Q = (float *)take(4 * L);
-  s->stage = (float *)take(4 * L);
+  s->stage = (float *)take(4 * (size_t)std::max<long long>(L, nM));
   s->ib = (float *)take(12 * L);
+  s->fb = (float2 *)take(24 * L);
+  s->nb = (uint8_t *)take(L);
+  s->Sz = (float *)take(4 * L);
   s->Om = damage ? (float *)take(4 * L) : nullptr;
   s->dOm = damage ? (float *)take(4 * L) : nullptr;
   s->M = (uint8_t *)take(L);
@@ -464,7 +518,7 @@ HeatDev make_dev(const mcb_heat_state *s, const mcb_heat_params *p) {
   h.nx = s->nx; h.ny = s->ny; h.nz = s->nz; h.nM = s->nM;
   h.T = s->T; h.A = s->A; h.M = s->M; h.c = s->c;
   h.Q = p->lightsOn ? s->Q : nullptr;
-  h.ib = s->ib; h.Omega = s->Om; h.dOmega = s->dOm; h.logA = s->logA; h.E = s->E;
+  h.ib = s->ib; h.fb = s->fb; h.nb = s->nb; h.Sz = s->Sz; h.Omega = s->Om; h.dOmega = s->dOm; h.logA = s->logA; h.E = s->E;
   h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0;
   h.dt = (float)p->dt; h.hdt = (float)(p->dt / 2); h.dtd = p->dt; h.base = s->base;
   h.nS = p->nSensors; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = s->sens; h.stepCounter = s->step;
@@ -562,7 +616,9 @@ mcb_status heat_stepper(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *
   const int grid = ctx->num_sms * 8;
   const long long L = s->L, nx = s->nx, ny = s->ny, nz = s->nz;
   if (s->factoredDt != p->dt || s->factoredHs != (int)(p->heatBoundaryType != 0)) {
-    for (int dir = 0; dir < 3; dir++) factor_kernel<<<grid, 128, 0, st>>>(h, dir, s->ib + (size_t)dir * L);
+    for (int dir = 0; dir < 3; dir++)
+      factor_kernel<<<grid, 128, 0, st>>>(h, dir, s->ib + (size_t)dir * L, s->fb + (size_t)dir * L);
+    neighbour_code_kernel<<<grid, 256, 0, st>>>(h, s->nb);
     MCB_CUDA(ctx, cudaGetLastError());
     s->factoredDt = p->dt;
     s->factoredHs = (int)(p->heatBoundaryType != 0);
@@ -740,6 +796,9 @@ void carve_static_state(ScratchCarve &c, mcb_heat_state *s, const mcb_heat_param
   s->Q = p->lightsOn ? (float *)c.take(4 * L) : nullptr;
   s->stage = (float *)c.take(4 * (size_t)std::max<long long>(L, nM));
   s->ib = (float *)c.take(12 * L);
+  s->fb = (float2 *)c.take(24 * L);
+  s->nb = (uint8_t *)c.take(L);
+  s->Sz = (float *)c.take(4 * L);
   s->Om = damage ? (float *)c.take(4 * L) : nullptr;
   s->dOm = damage ? (float *)c.take(4 * L) : nullptr;
   s->M = (uint8_t *)c.take(L);
@@ -769,7 +828,7 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
   if (measure.used > kHeatScratchBytes)
     return set_error(ctx, MCB_EINVAL,
                      "mcb_heat_forward_static: this grid needs %zu bytes of device scratch, more than its static "
-                     "limit of %zu bytes (about 37 bytes per voxel plus 8 per sensor and step); use mcb_heat_forward",
+                     "limit of %zu bytes (about 66 bytes per voxel plus 8 per sensor and step); use mcb_heat_forward",
                      measure.used, kHeatScratchBytes);
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
   void *base = nullptr;
@@ -807,31 +866,12 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
     MCB_CUDA(ctx, cudaMemcpyAsync(s.sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, st));
   }
   // step: factor the line matrices, clear the zero-start state, then plain launches per step
-  HeatDev h = make_dev(&s, p);
+  HeatStepper ks;
+  MCB_TRY(heat_stepper(ctx, &s, p, &ks));
+  const HeatDev &h = ks.h;
   const int grid = ctx->num_sms * 8;
-  for (int dir = 0; dir < 3; dir++) factor_kernel<<<grid, 128, 0, st>>>(h, dir, s.ib + (size_t)dir * L);
-  MCB_CUDA(ctx, cudaGetLastError());
-  MCB_CUDA(ctx, cudaMemsetAsync(s.maxEnc, 0, 4 * (size_t)nM, st));
-  MCB_CUDA(ctx, cudaMemsetAsync(s.step, 0, 16, st));
-  if (s.dOm) MCB_CUDA(ctx, cudaMemsetAsync(s.dOm, 0, 4 * (size_t)L, st));
-  const long long nx = s.nx, ny = s.ny, nz = s.nz;
-  const size_t smemX = x_smem((int)nx);
-  MCB_CUDA(ctx, cudaFuncSetAttribute(pass_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemX));
-  const int tw = s.tw;
-  if (tw == 32) MCB_TRY(setup_yz<32>(ctx, (int)ny, (int)nz));
-  else if (tw == 16) MCB_TRY(setup_yz<16>(ctx, (int)ny, (int)nz));
-  else MCB_TRY(setup_yz<8>(ctx, (int)ny, (int)nz));
-  const long long tilesX = ((ny + h.xl - 1) / h.xl) * nz;
-  const int gridX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * 64);
-  const long long tiles = ((nx + tw - 1) / tw) * std::max(ny, nz);
-  const int gridYZ = (int)std::min<long long>(tiles, (long long)ctx->num_sms * 64);
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
-  for (long long k = 0; k < nt; k++) {
-    pass_x_kernel<<<gridX, 256, smemX, st>>>(h);
-    if (tw == 32) launch_yz<32>(h, gridYZ, st);
-    else if (tw == 16) launch_yz<16>(h, gridYZ, st);
-    else launch_yz<8>(h, gridYZ, st);
-  }
+  for (long long k = 0; k < nt; k++) heat_step_launch(ks, st);
   if (nS) final_sensors_kernel<<<1, 128, 0, st>>>(h);
   if (s.dOm) merge_omega_kernel<<<grid, 256, 0, st>>>(s.Om, s.dOm, L);
   MCB_CUDA(ctx, cudaGetLastError());

@@ -19,6 +19,9 @@ struct HeatDev {
   const float *c;  // [nM x nM x 3]
   const float *Q;  // dTdt_abs or nullptr when the light is off
   const float *ib; // [3][L] inverse pivots
+  const float2 *fb;  // [3][L] scan multipliers {fm, bm} of every voxel's row
+  const uint8_t *nb; // [L] neighbourhood code (pass_x_kernel)
+  float *Sz;       // [L] z half-correction carried from the X pass to the Y pass
   float *Omega;    // or nullptr
   float *dOmega;   // damage accumulated during the current call, or nullptr
   const double *logA, *E;  // [nM]
@@ -59,16 +62,19 @@ __device__ __forceinline__ bool row_sinked(const HeatDev &h, bool lineSinked, in
 //   fm   forward multipliers  a_i / b'_{i-1}      (Thomas elimination d'_i = rhs_i + fm_i d'_{i-1})
 //   bm   backward multipliers cc_i / b'_i         (back substitution T_i = d'_i / b'_i + bm_i T_{i+1})
 //   ib   inverse pivots 1 / b'_i
+// fm and bm may be interleaved ({fm, bm} pairs): their element stride is fs * st.
 // Each recurrence is evaluated as a chunked warp scan of affine maps: every lane composes the
 // map of its contiguous chunk, a 5-step shuffle scan combines the lanes, and each lane then
 // replays its chunk from the carried-in value.
-static __device__ void warp_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
+static __device__ void warp_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
+                                  int fs = 1) {
+  const int sm = fs * st;
   const int lane = threadIdx.x & 31;
   const int k = (n + 31) >> 5;
   const int s = min(lane * k, n), e = min(s + k, n);
   float A = 0.f, B = 1.f;
   for (int i = s; i < e; i++) {
-    const float m = fm[i * st];
+    const float m = fm[i * sm];
     A = fmaf(m, A, rhs[i * st]);
     B *= m;
   }
@@ -84,13 +90,13 @@ static __device__ void warp_solve(float *rhs, const float *fm, const float *bm, 
   float d = __shfl_up_sync(0xffffffffu, A, 1);
   if (lane == 0) d = 0.f;
   for (int i = s; i < e; i++) {
-    d = fmaf(fm[i * st], d, rhs[i * st]);
+    d = fmaf(fm[i * sm], d, rhs[i * st]);
     rhs[i * st] = d;
   }
   A = 0.f;
   B = 1.f;
   for (int i = e - 1; i >= s; i--) {
-    const float f = bm[i * st];
+    const float f = bm[i * sm];
     A = fmaf(f, A, rhs[i * st] * ib[i * st]);
     B *= f;
   }
@@ -106,7 +112,7 @@ static __device__ void warp_solve(float *rhs, const float *fm, const float *bm, 
   float t = __shfl_down_sync(0xffffffffu, A, 1);
   if (lane == 31) t = 0.f;
   for (int i = e - 1; i >= s; i--) {
-    t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
+    t = fmaf(bm[i * sm], t, rhs[i * st] * ib[i * st]);
     rhs[i * st] = t;
   }
   __syncwarp();
@@ -116,7 +122,9 @@ static __device__ void warp_solve(float *rhs, const float *fm, const float *bm, 
 // holding K consecutive elements with fully unrolled chunk loops; 32/G lines are solved by a
 // warp at once. Requires n <= G*K.
 template <int K, int G>
-__device__ __forceinline__ void group_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st) {
+__device__ __forceinline__ void group_solve(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
+                                            int fs = 1) {
+  const int sm = fs * st;
   const int g = threadIdx.x & (G - 1);
   const int kk = (n + G - 1) / G;  // chunk length (<= K); odd lengths spread the lanes over banks
   const int s = g * kk;
@@ -126,7 +134,7 @@ __device__ __forceinline__ void group_solve(float *rhs, const float *fm, const f
   for (int j = 0; j < K; j++) {
     const int i = s + j;
     if (i < e) {
-      const float m = fm[i * st];
+      const float m = fm[i * sm];
       A = fmaf(m, A, rhs[i * st]);
       B *= m;
     }
@@ -146,7 +154,7 @@ __device__ __forceinline__ void group_solve(float *rhs, const float *fm, const f
   for (int j = 0; j < K; j++) {
     const int i = s + j;
     if (i < e) {
-      d = fmaf(fm[i * st], d, rhs[i * st]);
+      d = fmaf(fm[i * sm], d, rhs[i * st]);
       rhs[i * st] = d;
     }
   }
@@ -156,7 +164,7 @@ __device__ __forceinline__ void group_solve(float *rhs, const float *fm, const f
   for (int j = K - 1; j >= 0; j--) {
     const int i = s + j;
     if (i < e) {
-      const float f = bm[i * st];
+      const float f = bm[i * sm];
       A = fmaf(f, A, rhs[i * st] * ib[i * st]);
       B *= f;
     }
@@ -176,7 +184,7 @@ __device__ __forceinline__ void group_solve(float *rhs, const float *fm, const f
   for (int j = K - 1; j >= 0; j--) {
     const int i = s + j;
     if (i < e) {
-      t = fmaf(bm[i * st], t, rhs[i * st] * ib[i * st]);
+      t = fmaf(bm[i * sm], t, rhs[i * st] * ib[i * st]);
       rhs[i * st] = t;
     }
   }
@@ -190,28 +198,42 @@ __host__ __device__ constexpr int group_lanes(int n) { return n <= 128 ? 8 : (n 
 // stride st. Dispatches on the line length.
 template <int G>
 __device__ __forceinline__ void solve_lines_g(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
-                                              int lstride, int count) {
+                                              int lstride, int count, int fs) {
   constexpr int LPW = 32 / G;  // lines per warp at once
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int sub = (threadIdx.x & 31) / G;
   for (int l0 = warp * LPW; l0 < count; l0 += nw * LPW) {
     const int l = l0 + sub;
     // groups without a line run the same shuffles on an empty line so the warp stays converged
-    if (l < count) group_solve<16, G>(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
-    else group_solve<16, G>(rhs, fm, bm, ib, 0, st);
+    if (l < count)
+      group_solve<16, G>(rhs + l * lstride, fm + fs * l * lstride, bm + fs * l * lstride, ib + l * lstride, n, st, fs);
+    else group_solve<16, G>(rhs, fm, bm, ib, 0, st, fs);
   }
 }
 
+// Solves `count` lines; line l starts at element l * lstride, element stride st (fm and bm:
+// fs times both strides, fs = 2 for interleaved {fm, bm} pairs).
 __device__ __forceinline__ void solve_lines(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
-                                            int lstride, int count) {
+                                            int lstride, int count, int fs = 1) {
   const int G = group_lanes(n);
-  if (G == 8) solve_lines_g<8>(rhs, fm, bm, ib, n, st, lstride, count);
-  else if (G == 16) solve_lines_g<16>(rhs, fm, bm, ib, n, st, lstride, count);
-  else if (G == 32) solve_lines_g<32>(rhs, fm, bm, ib, n, st, lstride, count);
+  if (G == 8) solve_lines_g<8>(rhs, fm, bm, ib, n, st, lstride, count, fs);
+  else if (G == 16) solve_lines_g<16>(rhs, fm, bm, ib, n, st, lstride, count, fs);
+  else if (G == 32) solve_lines_g<32>(rhs, fm, bm, ib, n, st, lstride, count, fs);
   else {
     for (int l = threadIdx.x >> 5; l < count; l += blockDim.x >> 5)
-      warp_solve(rhs + l * lstride, fm + l * lstride, bm + l * lstride, ib + l * lstride, n, st);
+      warp_solve(rhs + l * lstride, fm + fs * l * lstride, bm + fs * l * lstride, ib + l * lstride, n, st, fs);
   }
 }
+
+// Asynchronous global -> shared copies (cp.async, no registers held while in flight).
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 }  // namespace mcb

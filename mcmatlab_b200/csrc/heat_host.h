@@ -15,7 +15,9 @@ struct mcb_heat_state {
   double factoredDt = -1.0;
   int factoredHs = -1;
   float *T = nullptr, *A = nullptr, *Q = nullptr, *ib = nullptr, *Om = nullptr, *dOm = nullptr, *stage = nullptr,
-        *c = nullptr;
+        *c = nullptr, *Sz = nullptr;
+  float2 *fb = nullptr;
+  uint8_t *nb = nullptr;
   uint8_t *M = nullptr;
   double *logA = nullptr, *E = nullptr;
   unsigned int *maxEnc = nullptr;

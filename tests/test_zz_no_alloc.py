@@ -58,7 +58,7 @@ def test_static_entry_allocates_no_device_memory():
 
 def test_static_entry_rejects_grids_beyond_its_scratch():
     from mcmatlab_b200 import native
-    big = heatcases._base(100, 5, 0, True, 1, 0.9, True)  # 1e6 voxels x 37 B > 32 MiB
+    big = heatcases._base(100, 5, 0, True, 1, 0.9, True)  # 1e6 voxels x 66 B > 32 MiB
     with pytest.raises(native.MCBError, match="static limit"):
         native.heat_forward_static(big["T0"], big["Omega0"], big["hp"], 100, 100, 100)
     # the context stays usable, and the same grid runs through the allocating entry
