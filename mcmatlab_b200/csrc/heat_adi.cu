@@ -371,8 +371,8 @@ namespace {
 using namespace mcb;
 
 // Widest tile that keeps two blocks per SM (<= 100 KB each), else one block (<= 200 KB).
+// (16-wide tiles measured faster than 32-wide ones on the 100^3 grid: twice the blocks)
 int yz_tile_width(int n) {
-  if (yz_tile_bytes<32>(n) <= 100000) return 32;
   if (yz_tile_bytes<16>(n) <= 100000) return 16;
   if (yz_tile_bytes<8>(n) <= 200000) return 8;
   return 0;
@@ -384,9 +384,10 @@ size_t yz_smem(int TW, int n) {
 
 size_t x_smem_lines(int nx, int xl) { return (size_t)xl * 5 * 4 * (nx + 1) + 64; }
 
-// x-lines per X-pass block: the most that keeps the block's shared memory within 100 KB
+// x-lines per X-pass block: at most 8 (more, smaller blocks measured faster on 300-long lines),
+// fewer if the block's shared memory would exceed 100 KB
 int x_lines(int nx) {
-  for (int xl = 32; xl >= 2; xl >>= 1)
+  for (int xl = 8; xl >= 2; xl >>= 1)
     if (x_smem_lines(nx, xl) <= 100000) return xl;
   return x_smem_lines(nx, 1) <= 200000 ? 1 : 0;
 }

@@ -191,12 +191,10 @@ __device__ __forceinline__ void group_solve(float *rhs, const float *fm, const f
   __syncwarp();
 }
 
-// Lanes per line for the grouped solver (0: use the one-warp-per-line solver).
-__host__ __device__ constexpr int group_lanes(int n) { return n <= 128 ? 8 : (n <= 256 ? 16 : (n <= 512 ? 32 : 0)); }
 
 // Solves `count` lines of one tile; line l starts at base + l*lstride (elements), element
 // stride st. Dispatches on the line length.
-template <int G>
+template <int K, int G>
 __device__ __forceinline__ void solve_lines_g(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
                                               int lstride, int count, int fs) {
   constexpr int LPW = 32 / G;  // lines per warp at once
@@ -206,19 +204,21 @@ __device__ __forceinline__ void solve_lines_g(float *rhs, const float *fm, const
     const int l = l0 + sub;
     // groups without a line run the same shuffles on an empty line so the warp stays converged
     if (l < count)
-      group_solve<16, G>(rhs + l * lstride, fm + fs * l * lstride, bm + fs * l * lstride, ib + l * lstride, n, st, fs);
-    else group_solve<16, G>(rhs, fm, bm, ib, 0, st, fs);
+      group_solve<K, G>(rhs + l * lstride, fm + fs * l * lstride, bm + fs * l * lstride, ib + l * lstride, n, st, fs);
+    else group_solve<K, G>(rhs, fm, bm, ib, 0, st, fs);
   }
 }
 
 // Solves `count` lines; line l starts at element l * lstride, element stride st (fm and bm:
-// fs times both strides, fs = 2 for interleaved {fm, bm} pairs).
+// fs times both strides, fs = 2 for interleaved {fm, bm} pairs). Lines up to 128 use groups of
+// 16 lanes holding 8 elements each, up to 256 16 lanes of 16, up to 512 32 lanes of 16, longer
+// lines one warp each (16-lane groups measured faster than 8- and 32-lane groups on 100-long
+// lines).
 __device__ __forceinline__ void solve_lines(float *rhs, const float *fm, const float *bm, const float *ib, int n, int st,
                                             int lstride, int count, int fs = 1) {
-  const int G = group_lanes(n);
-  if (G == 8) solve_lines_g<8>(rhs, fm, bm, ib, n, st, lstride, count, fs);
-  else if (G == 16) solve_lines_g<16>(rhs, fm, bm, ib, n, st, lstride, count, fs);
-  else if (G == 32) solve_lines_g<32>(rhs, fm, bm, ib, n, st, lstride, count, fs);
+  if (n <= 128) solve_lines_g<8, 16>(rhs, fm, bm, ib, n, st, lstride, count, fs);
+  else if (n <= 256) solve_lines_g<16, 16>(rhs, fm, bm, ib, n, st, lstride, count, fs);
+  else if (n <= 512) solve_lines_g<16, 32>(rhs, fm, bm, ib, n, st, lstride, count, fs);
   else {
     for (int l = threadIdx.x >> 5; l < count; l += blockDim.x >> 5)
       warp_solve(rhs + l * lstride, fm + fs * l * lstride, bm + fs * l * lstride, ib + l * lstride, n, st, fs);
