@@ -242,6 +242,12 @@ def run_ours(args):
                "steps_per_s": steps_mc / (mc_ms / 1e3),
                "parallelism": "packets sharded over %d ranks, one NCCL all-reduce of the tallies" % ws if ws > 1 else "1 GPU"},
     }
+    # transport roofline: propagation sub-steps/s against the measured scattered FP64 atomicAdd
+    # rate (one deposit per sub-step is the algorithmic work; runs in one voxel share one atomic)
+    atom = native.probe_atomics(1 << 20, device=dev)
+    res["mc"]["roofline"] = {"bound": "fp64 atomics", "achieved": steps_mc / (mc_ms / 1e3), "peak": atom,
+                             "unit": "sub-steps/s vs FP64 atomicAdd/s", "frac": steps_mc / (mc_ms / 1e3) / atom,
+                             "peak_source": "measured in this run: mcb_probe_atomics, 2^20 scattered slots"}
     # the remaining measurements are single-GPU ones (run on 1-GPU invocations only)
     if args.c2 and ws == 1:
         res["mc_batched"] = batched_sweep_measure(dev, args.c2_instances, args.c2_scale)
@@ -252,6 +258,7 @@ def run_ours(args):
     if rank == 0:
         if args.cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
+            res["mc"]["cpu_baseline"] = res["cpu_baseline"].pop("mc")
         print(json.dumps(res), flush=True)
     state.close()
     if dist:
@@ -327,12 +334,19 @@ def adjoint_measure(dev, nt):
             "adjoint_over_forward": (g["forwardMs"] + g["adjointMs"]) / fwd_ms}
 
 
-def reference_setup():
+REF_MC_PACKETS = 1e5
+
+
+def reference_setup(timings=None):
     from oracle import ref
-    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=1e5, seed=1)
+    m = configs.standard_tissue_cube(n=N_GRID, nPhotons=REF_MC_PACKETS, seed=1)
     mc_in = mexargs.prepare_mc(m)
     tree = mexargs.mex_model_tree(mc_in)
+    t0 = time.perf_counter()
     out = ref.RefMC().run(tree, seed=None)  # reference MC, all cores, for the heat source
+    if timings is not None:
+        timings["mc_s"] = time.perf_counter() - t0
+        timings["mc_packets"] = float(np.asarray(out["nPhotons"]).ravel()[0])
     NFR = out["NFR"]
     NFR = NFR[..., 0] if NFR.ndim == 4 else NFR
     mua = mc_in["mua"][:, 0]
@@ -343,7 +357,8 @@ def reference_setup():
 def cpu_baseline(args, sample_steps):
     """The reference's own heat stepper on all host cores, bounded sample of `sample_steps` steps."""
     from oracle import ref
-    m, NA = reference_setup()
+    tm = {}
+    m, NA = reference_setup(tm)
     th, c, Q, dt = build_heat_inputs(NA, m)
     hp = mexargs.heat_mex_params(th["M"], th["A"], th["E"], c, Q, True, 0, None, None, True, sample_steps, dt)
     T0 = np.full((N_GRID,) * 3, 37.0, np.float32, order="F")
@@ -356,7 +371,10 @@ def cpu_baseline(args, sample_steps):
     dtw = time.perf_counter() - t0
     return {"value": N_GRID ** 3 * sample_steps / dtw, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
             "sample": "%d DG-ADI steps of the same 100^3 workload (light on, damage), reference MEX C code "
-                      "(-Ofast -fopenmp) on %d host threads" % (sample_steps, cores)}
+                      "(-Ofast -fopenmp) on %d host threads" % (sample_steps, cores),
+            "mc": {"value": tm["mc_packets"] / tm["mc_s"], "unit": "photon packets/s", "cores": cores, "kind": "reference",
+                   "sample": "%.0e packets of the 100^3 standard-tissue cube (MCmatlab.c, -Ofast -fopenmp, %d threads)"
+                             % (tm["mc_packets"], cores)}}
 
 
 def run_reference(args):

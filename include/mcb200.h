@@ -245,6 +245,11 @@ MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, cons
 MCB_API mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
                                            double *sensorTemps, float *maxMediaTemps);
 
+/* No counterpart in the reference: measures the device's FP64 atomicAdd throughput to
+ * scattered addresses of a buffer of `slots` doubles (the transport's roofline denominator:
+ * one FP64 deposit per propagation sub-step). */
+MCB_API mcb_status mcb_probe_atomics(mcb_ctx *ctx, int64_t slots, double *atomicsPerSecond);
+
 /* No counterpart in the reference: device time in milliseconds (CUDA events on the context's
  * stream) of the transport kernel or stepping loop of the last call on this context. */
 MCB_API double mcb_last_kernel_ms(const mcb_ctx *ctx);

@@ -95,3 +95,40 @@ extern "C" mcb_status mcb_ctx_destroy(mcb_ctx *ctx) {
 extern "C" const char *mcb_last_error(const mcb_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
 extern "C" volatile int *mcb_cancel_flag(mcb_ctx *ctx) { return ctx ? ctx->cancel_host : nullptr; }
+
+namespace {
+
+// Scattered FP64 atomicAdd throughput: every thread adds to pseudo-random slots of a buffer
+// (xorshift64 sequence per thread, multiplicative hash to a slot).
+__global__ void atomic_probe_kernel(double *buf, unsigned long long slots, int perThread) {
+  unsigned long long x = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x + 1) * 0x9E3779B97F4A7C15ull;
+  for (int k = 0; k < perThread; k++) {
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    atomicAdd(buf + (x * 0x2545F4914F6CDD1Dull) % slots, 1.0);
+  }
+}
+
+}  // namespace
+
+extern "C" mcb_status mcb_probe_atomics(mcb_ctx *ctx, int64_t slots, double *atomicsPerSecond) {
+  using namespace mcb;
+  if (!ctx) return MCB_EINVAL;
+  if (slots < 1 || !atomicsPerSecond) return set_error(ctx, MCB_EINVAL, "slots must be >= 1");
+  MCB_CUDA(ctx, cudaSetDevice(ctx->device));
+  void *buf = nullptr;
+  MCB_TRY(pool_get(ctx, SLOT_PROBE, 8 * (size_t)slots, &buf));
+  const int grid = ctx->num_sms * 8, threads = 256, perThread = 256;
+  MCB_CUDA(ctx, cudaMemsetAsync(buf, 0, 8 * (size_t)slots, ctx->stream));
+  atomic_probe_kernel<<<grid, threads, 0, ctx->stream>>>((double *)buf, (unsigned long long)slots, perThread);
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  atomic_probe_kernel<<<grid, threads, 0, ctx->stream>>>((double *)buf, (unsigned long long)slots, perThread);
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  MCB_CUDA(ctx, cudaGetLastError());
+  MCB_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  MCB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  *atomicsPerSecond = (double)grid * threads * perThread / (ms * 1e-3);
+  return MCB_OK;
+}

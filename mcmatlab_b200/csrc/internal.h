@@ -74,6 +74,7 @@ enum PoolSlot {
   SLOT_HEAT_MISC,
   SLOT_HEAT_SENS,
   SLOT_HEAT_ADJ,
+  SLOT_PROBE,
   SLOT_BATCH_BASE = 40
 };
 

@@ -24,7 +24,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
           6: "MCB_ELAUNCH"}
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
-           "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint",
+           "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint", "mcb_probe_atomics",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -66,6 +66,7 @@ def lib():
                                               C.POINTER(C.c_float)]
             L.mcb_heat_state_read.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
             L.mcb_heat_state_destroy.argtypes = [C.c_void_p]
+            L.mcb_probe_atomics.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
             L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
             L.mcb_last_kernel_ms.restype = C.c_double
             _lib = L
@@ -185,6 +186,14 @@ def heat_adjoint(T0, hp, nx, ny, nz, damageWeight=None, peakWeight=None, nCheckp
     return dict(J=g.J, J_damage=g.J_damage, J_peak=g.J_peak, dJ_dc=dc.reshape(nM, nM, 3, order="F"),
                 dJ_dQ=dQ.reshape(shp, order="F"), dJ_dT0=dT.reshape(shp, order="F"),
                 forwardMs=g.forwardMs, adjointMs=g.adjointMs)
+
+
+def probe_atomics(slots=1 << 20, device=0):
+    """FP64 atomicAdd operations per second to scattered slots of a `slots`-double buffer."""
+    ctx = context(device)
+    r = C.c_double()
+    _check(lib().mcb_probe_atomics(ctx, int(slots), C.byref(r)), ctx)
+    return r.value
 
 
 def last_kernel_ms(device=0):
