@@ -84,7 +84,6 @@ __global__ void factor_kernel(HeatDev h, int dir, float *ibOut, float2 *fbOut) {
 
 // Neighbourhood code of every voxel (once per call): bit 2d (2d+1) is set when the lower
 // (upper) neighbour along d is missing or of another medium; kNbSink marks heat-sinked voxels.
-constexpr int kNbSink = 64;
 __global__ void neighbour_code_kernel(HeatDev h, uint8_t *out) {
   const long long sxy = (long long)h.nx * h.ny, L = sxy * h.nz;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
@@ -175,6 +174,8 @@ __global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
   const float *ibx = h.ib;
   const float2 *fbx = h.fb;
   const int yTiles = (ny + XL - 1) / XL;
+  // e / nx as a multiply-high by ceil(2^32 / nx): exact while e * nx < 2^32 (e < XL * nx here)
+  const unsigned mag = 0xFFFFFFFFu / (unsigned)nx + 1u;
   for (int tile = blockIdx.x; tile < yTiles * nz; tile += gridDim.x) {
     const int y0 = (tile % yTiles) * XL, iz = tile / yTiles;
     const int cnt = min(XL, ny - y0);
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
       for (int u = 0; u < U; u++) {
         const int e = e0 + u * blockDim.x;
         if (e < total) {
-          const int l = e / nx, x = e - l * nx;
+          const int l = (int)__umulhi((unsigned)e, mag), x = e - l * nx;
           const int v = x + (y0 + l) * nx + iz * sxy;
           voxel_load(h, v, x, y0 + l, iz, in[u]);
           vi[u] = ibx[v];
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
       for (int u = 0; u < U; u++) {
         const int e = e0 + u * blockDim.x;
         if (e < total) {
-          const int l = e / nx, x = e - l * nx;
+          const int l = (int)__umulhi((unsigned)e, mag), x = e - l * nx;
           const int v = x + (y0 + l) * nx + iz * sxy;
           float r, hy, hz;
           voxel_explicit(h, v, x, y0 + l, iz, in[u], r, hy, hz);
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
     solve_lines(rhs, fm, bm, ib, nx, 1, P, cnt);
     __syncthreads();
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int l = e / nx, x = e - l * nx;
+      const int l = (int)__umulhi((unsigned)e, mag), x = e - l * nx;
       h.A[x + (y0 + l) * nx + iz * sxy] = rhs[l * P + x] - sy[l * P + x];
     }
     __syncthreads();

@@ -57,29 +57,29 @@ struct AdjDev {
   int step;          // n + 1 of the step being reversed
 };
 
-__device__ __forceinline__ void vox_coords(const HeatDev &h, long long v, int &ix, int &iy, int &iz) {
-  const long long sxy = (long long)h.nx * h.ny;
-  iz = (int)(v / sxy);
-  const long long r = v - (long long)iz * sxy;
-  iy = (int)(r / h.nx);
-  ix = (int)(r - (long long)iy * h.nx);
-}
-
+// The grid-wide adjoint kernels walk x-rows: block b takes rows b, b + gridDim.x, ... (row =
+// iy + ny * iz) and its threads the x positions of a row, so no voxel index is divided.
 // out = U - dt/2 D_dir (U - T^n): dir 2 gives A2 from U = T^{n+1}, dir 1 gives A1 from U = A2.
 __global__ void adj_recon_kernel(AdjDev a, int dir) {
   const HeatDev &h = a.h;
   const float *U = dir == 2 ? a.Tp : a.A2;
   float *out = dir == 2 ? a.A2 : a.A1;
-  const long long L = (long long)h.nx * h.ny * h.nz;
   const long long st = dir == 1 ? h.nx : (long long)h.nx * h.ny;
   const int n = dir == 1 ? h.ny : h.nz;
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
-    int ix, iy, iz;
-    vox_coords(h, v, ix, iy, iz);
+  const int rows = h.ny * h.nz;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x)
+  for (int ix = threadIdx.x; ix < h.nx; ix += blockDim.x) {
+    const int iy = row % h.ny, iz = row / h.ny;
+    const long long v = ix + (long long)row * h.nx;
     const int pos = dir == 1 ? iy : iz;
     const float u = U[v];
     float d = 0.f;
-    if (!sinked(h, ix, iy, iz)) {
+    const int code = h.nb[v];
+    if (!(code & kNbSink) && (code & (dir == 1 ? 12 : 48)) == 0) {
+      // both line neighbours exist and share the medium: one coefficient
+      const float w = u - a.Tn[v];
+      d = cf(h, h.M[v], h.M[v], dir) * ((U[v - st] - a.Tn[v - st]) + (U[v + st] - a.Tn[v + st]) - 2.f * w);
+    } else if (!sinked(h, ix, iy, iz)) {
       const float w = u - a.Tn[v];
       const int mi = h.M[v];
       if (pos > 0) d += cf(h, mi, h.M[v - st], dir) * ((U[v - st] - a.Tn[v - st]) - w);
@@ -122,7 +122,7 @@ __global__ void adj_damage_tail_kernel(AdjDev a) {
 }
 
 // X^T solve: rho1 = X^-T rho2. Same tiling as the forward X pass (h.xl lines per block).
-__global__ void __launch_bounds__(256) adj_solve_x_kernel(AdjDev a) {
+__global__ void __launch_bounds__(256, 3) adj_solve_x_kernel(AdjDev a) {
   extern __shared__ unsigned char smem[];
   const HeatDev &h = a.h;
   const int nx = h.nx, ny = h.ny, nz = h.nz;
@@ -173,7 +173,7 @@ __host__ __device__ constexpr size_t adj_yz_tile_bytes(int n) {
 // Y^T / Z^T solves: rho2 = Y^-T rho3 (ZPASS false), rho3 = Z^-T lambda' (ZPASS true). Same
 // tiling as the forward Y/Z passes: TW consecutive x positions, one line per x.
 template <int TW, bool ZPASS>
-__global__ void __launch_bounds__(256) adj_solve_yz_kernel(AdjDev a) {
+__global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
   extern __shared__ unsigned char smem[];
   constexpr int P = TW + 1;
   const HeatDev &h = a.h;
@@ -239,26 +239,53 @@ __global__ void __launch_bounds__(256) adj_assemble_kernel(AdjDev a) {
   const int nM = h.nM, nM2 = nM * nM;
   for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) sdc[k] = 0.0;
   __syncthreads();
-  const long long L = (long long)h.nx * h.ny * h.nz;
   const long long sxy = (long long)h.nx * h.ny;
   const float dt = h.dt, hdt = h.hdt;
   // same-medium faces (the common case) accumulate in registers, flushed when the medium changes
   int curM = -1;
-  double same[3] = {0.0, 0.0, 0.0};
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
-    int ix, iy, iz;
-    vox_coords(h, v, ix, iy, iz);
+  float same[3] = {0.f, 0.f, 0.f};
+  const int rows = h.ny * h.nz;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x)
+  for (int ix = threadIdx.x; ix < h.nx; ix += blockDim.x) {
+    const int iy = row % h.ny, iz = row / h.ny;
+    const long long v = ix + (long long)row * h.nx;
     const int mv = h.M[v];
     const bool nsv = !sinked(h, ix, iy, iz);
     const float r1v = a.r1[v], r2v = a.r2[v], r3v = a.r3[v];
     const float tv = a.Tn[v];
     if (nsv && mv != curM) {
       if (curM >= 0)
-        for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], same[d]);
+        for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
       curM = mv;
-      same[0] = same[1] = same[2] = 0.0;
+      same[0] = same[1] = same[2] = 0.f;
     }
     float lam = r1v;
+    // interior of a homogeneous region with no heat-sinked neighbour: all six faces share one
+    // coefficient per direction, every load is independent of the others
+    const bool interior = h.nb[v] == 0 && !(h.hs && (ix <= 1 || ix >= h.nx - 2 || iy <= 1 || iy >= h.ny - 2 ||
+                                                     iz <= 1 || iz >= h.nz - 2));
+    if (interior) {
+      const long long sy = h.nx, sz = sxy;
+      const float cx = cf(h, mv, mv, 0), cy = cf(h, mv, mv, 1), cz = cf(h, mv, mv, 2);
+      const float r1xl = a.r1[v - 1], r1xr = a.r1[v + 1], r1yl = a.r1[v - sy], r1yr = a.r1[v + sy];
+      const float r1zl = a.r1[v - sz], r1zr = a.r1[v + sz];
+      const float r2yl = a.r2[v - sy], r2yr = a.r2[v + sy], r3zl = a.r3[v - sz], r3zr = a.r3[v + sz];
+      const float txl = a.Tn[v - 1], txr = a.Tn[v + 1], tyl = a.Tn[v - sy], tyr = a.Tn[v + sy];
+      const float tzl = a.Tn[v - sz], tzr = a.Tn[v + sz];
+      const float a1v = a.A1[v], a1l = a.A1[v - 1], a1r = a.A1[v + 1];
+      const float a2v = a.A2[v], a2l = a.A2[v - sy], a2r = a.A2[v + sy];
+      const float tpv = a.Tp[v], tpl = a.Tp[v - sz], tpr = a.Tp[v + sz];
+      const float qy = dt * r1v - hdt * r2v, qz = dt * r1v - hdt * r3v;
+      lam += cx * hdt * (r1xl + r1xr - 2.f * r1v) +
+             cy * ((dt * r1yl - hdt * r2yl) + (dt * r1yr - hdt * r2yr) - 2.f * qy) +
+             cz * ((dt * r1zl - hdt * r3zl) + (dt * r1zr - hdt * r3zr) - 2.f * qz);
+      same[0] += hdt * r1v * ((txl + a1l) + (txr + a1r) - 2.f * (tv + a1v));
+      same[1] += dt * r1v * (tyl + tyr - 2.f * tv) + hdt * r2v * ((a2l - tyl) + (a2r - tyr) - 2.f * (a2v - tv));
+      same[2] += dt * r1v * (tzl + tzr - 2.f * tv) + hdt * r3v * ((tpl - tzl) + (tpr - tzr) - 2.f * (tpv - tv));
+      a.lamOut[v] = lam;
+      if (a.dQ) a.dQ[v] += dt * r1v;
+      continue;
+    }
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       const int pos = d == 0 ? ix : (d == 1 ? iy : iz);
@@ -285,7 +312,7 @@ __global__ void __launch_bounds__(256) adj_assemble_kernel(AdjDev a) {
           if (d == 0) contrib = hdt * r1v * ((tu + a.A1[u]) - pv);
           else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((a.A2[u] - tu) - pv);
           else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((a.Tp[u] - tu) - pv);
-          if (mu == mv) same[d] += (double)contrib;
+          if (mu == mv) same[d] += contrib;
           else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
         }
       }
@@ -294,7 +321,7 @@ __global__ void __launch_bounds__(256) adj_assemble_kernel(AdjDev a) {
     if (a.dQ && nsv) a.dQ[v] += dt * r1v;
   }
   if (curM >= 0)
-    for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], same[d]);
+    for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
   __syncthreads();
   for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x)
     if (sdc[k] != 0.0) atomicAdd(&a.dc[k], sdc[k]);
@@ -465,7 +492,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   else rc = adj_setup_yz<8>(ctx, ny, nz);
   if (rc != MCB_OK) return fail(rc);
   const int gridX = ks.gridX, gridYZ = ks.gridYZ;
-  const int gridE = ctx->num_sms * 8;
+  const int gridE = (int)std::min<long long>((long long)ny * nz, (long long)ctx->num_sms * 16);
+  const int rowThreads = nx <= 128 ? 128 : 256;
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
 
   // forward sweep: checkpoints every K steps, running maxima of the peak list
@@ -499,8 +527,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       a.lamOut = lamNext;
       a.step = (int)(n + 1);
       if (nD || nP) adj_seed_kernel<<<gridL, 256, 0, st>>>(a);
-      adj_recon_kernel<<<gridE, 256, 0, st>>>(a, 2);
-      adj_recon_kernel<<<gridE, 256, 0, st>>>(a, 1);
+      adj_recon_kernel<<<gridE, rowThreads, 0, st>>>(a, 2);
+      adj_recon_kernel<<<gridE, rowThreads, 0, st>>>(a, 1);
       if (tw == 32) adj_launch_yz<32>(a, true, gridYZ, st);
       else if (tw == 16) adj_launch_yz<16>(a, true, gridYZ, st);
       else adj_launch_yz<8>(a, true, gridYZ, st);
@@ -508,7 +536,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       else if (tw == 16) adj_launch_yz<16>(a, false, gridYZ, st);
       else adj_launch_yz<8>(a, false, gridYZ, st);
       adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
-      adj_assemble_kernel<<<gridE, 256, 0, st>>>(a);
+      adj_assemble_kernel<<<gridE, rowThreads, 0, st>>>(a);
       if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
       std::swap(lam, lamNext);
     }

@@ -37,6 +37,8 @@ struct HeatDev {
   int xl;  // x-lines per block in the X pass
 };
 
+constexpr int kNbSink = 64;  // neighbourhood-code bit of heat-sinked voxels (neighbour_code_kernel)
+
 __device__ __forceinline__ unsigned int enc_max(float f) {
   const unsigned int b = __float_as_uint(f);
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
