@@ -45,7 +45,7 @@ sys.path.insert(0, ROOT)
 from mcmatlab_b200 import configs, mexargs, prep  # noqa: E402
 
 METRIC = "photon packets/s, heat voxel-updates/s on 1 B200; batched+adjoint vs plain"
-HEAT_STEP_DRAM_BYTES = 39.4e6
+HEAT_STEP_DRAM_BYTES = 60.0e6
 N_GRID = 100
 MC_PACKETS = 1_000_000
 
