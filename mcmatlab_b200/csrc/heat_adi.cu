@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256, 3) pass_x_kernel(HeatDev h) {
     const int y0 = (tile % yTiles) * XL, iz = tile / yTiles;
     const int cnt = min(XL, ny - y0);
     const int total = cnt * nx;
-    constexpr int U = 4;
+    constexpr int U = 2;  // elements in flight per thread (4 measured slower: register spills)
     for (int e0 = threadIdx.x; e0 < total; e0 += blockDim.x * U) {
       VoxIn in[U];
       float vi[U];

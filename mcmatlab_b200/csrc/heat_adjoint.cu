@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
 }
 
 // lambda^n, dJ/dQ and dJ/dc of one reversed step (7-point stencil over every voxel).
-__global__ void __launch_bounds__(256) adj_assemble_kernel(AdjDev a) {
+__global__ void __launch_bounds__(512) adj_assemble_kernel(AdjDev a) {
   const HeatDev &h = a.h;
   __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
   const int nM = h.nM, nM2 = nM * nM;
@@ -493,7 +493,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   if (rc != MCB_OK) return fail(rc);
   const int gridX = ks.gridX, gridYZ = ks.gridYZ;
   const int gridE = (int)std::min<long long>((long long)ny * nz, (long long)ctx->num_sms * 16);
-  const int rowThreads = nx <= 128 ? 128 : 256;
+  // one thread per x position of a row (a warp multiple, at most 512): no idle second pass
+  const int rowThreads = std::min(512, (nx + 31) / 32 * 32);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
 
   // forward sweep: checkpoints every K steps, running maxima of the peak list
