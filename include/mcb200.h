@@ -245,6 +245,19 @@ MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, cons
 MCB_API mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
                                            double *sensorTemps, float *maxMediaTemps);
 
+/* Interface normals for mismatched refractive indices, on the device. No counterpart in the
+ * reference's C code: its MATLAB host computes them before the MEX call
+ * (getOpticalMediaProperties.m:222-244, imgradientxyz + smoothn). M1 [nx*ny*nz] holds 1-based
+ * media; riClass [nM] the refractive-index class (0..nClass-1) of every medium (media with equal
+ * refractive-index rows share a class). Per class, the 3D Sobel gradient of the class indicator
+ * divided by the voxel size, smoothed when smoothingLengthScale > 0 with smoothness
+ * s = max(1, round(smoothingLengthScale / max(dx, dy, dz))), is written into the class's voxels;
+ * thetaPhi [2 x nx*ny*nz] (column-major, as the MC model's interfaceNormals) receives
+ * theta = pi/2 - elevation and phi = azimuth. Smoothing needs every axis <= 1024 voxels. */
+MCB_API mcb_status mcb_interface_normals(mcb_ctx *ctx, int32_t nx, int32_t ny, int32_t nz, const uint8_t *M1, int32_t nM,
+                                         const int32_t *riClass, int32_t nClass, double dx, double dy, double dz,
+                                         double smoothingLengthScale, float *thetaPhi);
+
 /* No counterpart in the reference: measures the device's FP64 atomicAdd throughput to
  * scattered addresses of a buffer of `slots` doubles (the transport's roofline denominator:
  * one FP64 deposit per propagation sub-step). */

@@ -75,6 +75,7 @@ enum PoolSlot {
   SLOT_HEAT_SENS,
   SLOT_HEAT_ADJ,
   SLOT_PROBE,
+  SLOT_NORMALS,
   SLOT_BATCH_BASE = 40
 };
 

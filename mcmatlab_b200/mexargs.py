@@ -49,7 +49,8 @@ def prepare_mc(mdl, simType=1):
     if MC.useLightCollector and MC.boundaryType == 0:
         raise ValueError("Error: If boundaryType == 0, no photons can escape to be registered on the light collector. Disable light collector or change boundaryType.")
     media = G.mediaPropertiesFunc(G.mediaPropParams)
-    mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC)
+    mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC,
+                                       MC.smoothingLengthScale)
     SD = MC.sourceDistribution
     if np.ndim(SD) == 0:
         sd = None

@@ -25,6 +25,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
            "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint", "mcb_probe_atomics",
+           "mcb_interface_normals",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -67,6 +68,9 @@ def lib():
             L.mcb_heat_state_read.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]
             L.mcb_heat_state_destroy.argtypes = [C.c_void_p]
             L.mcb_probe_atomics.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
+            L.mcb_interface_normals.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint8),
+                                                C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
+                                                C.c_double, C.c_double, C.POINTER(C.c_float)]
             L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
             L.mcb_last_kernel_ms.restype = C.c_double
             _lib = L
@@ -186,6 +190,24 @@ def heat_adjoint(T0, hp, nx, ny, nz, damageWeight=None, peakWeight=None, nCheckp
     return dict(J=g.J, J_damage=g.J_damage, J_peak=g.J_peak, dJ_dc=dc.reshape(nM, nM, 3, order="F"),
                 dJ_dQ=dQ.reshape(shp, order="F"), dJ_dT0=dT.reshape(shp, order="F"),
                 forwardMs=g.forwardMs, adjointMs=g.adjointMs)
+
+
+def interface_normals(M1, n_per_submedium, dx, dy, dz, smoothingLengthScale=0.0, device=0):
+    """prep.interface_normals on the device (mcb_interface_normals): (theta, phi) float32 [2, L]."""
+    ctx = context(device)
+    M = np.ascontiguousarray(np.asarray(M1, dtype=np.uint8).reshape(-1, order="F"))
+    nrows = np.asarray(n_per_submedium, dtype=np.float64)
+    if nrows.ndim == 1:
+        nrows = nrows[:, None]
+    uniq, inv = np.unique(nrows, axis=0, return_inverse=True)
+    cls = np.ascontiguousarray(np.asarray(inv, dtype=np.int32).reshape(-1))
+    nx, ny, nz = np.shape(M1)
+    out = np.empty(2 * M.size, dtype=np.float32)
+    _check(lib().mcb_interface_normals(ctx, nx, ny, nz, M.ctypes.data_as(C.POINTER(C.c_uint8)), cls.size,
+                                       cls.ctypes.data_as(C.POINTER(C.c_int32)), int(uniq.shape[0]), float(dx),
+                                       float(dy), float(dz), float(smoothingLengthScale),
+                                       out.ctypes.data_as(C.POINTER(C.c_float))), ctx)
+    return out.reshape(2, M.size, order="F")
 
 
 def probe_atomics(slots=1 << 20, device=0):

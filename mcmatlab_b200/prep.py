@@ -7,8 +7,8 @@ here in numpy, each citing the MATLAB function it follows:
 * geometry evaluation           +MCmatlab/@geometry/geometry.m:44-66, :130-138
 * optical media properties      +MCmatlab/@model/private/getOpticalMediaProperties.m:1-258
 * Sobel interface normals       +MCmatlab/@model/private/imgradientxyz.m:38-59 and
-                                getOpticalMediaProperties.m:222-244 (the branch without
-                                smoothn smoothing, :232-233)
+                                getOpticalMediaProperties.m:222-244, with the smoothn
+                                smoothing of the gradients (:230-231; smooth_gradients)
 * thermal media properties      +MCmatlab/@model/private/getThermalMediaProperties.m
 * dT/dt arrays, dt limit        +MCmatlab/@model/simulateHeatDistribution.m:469-514
 * temperature sensor weights    +MCmatlab/@model/simulateHeatDistribution.m:543-609
@@ -110,12 +110,34 @@ def sobel_gradients(I):
     return out[0], out[1], out[2]
 
 
-def interface_normals(M1, n_per_submedium, dx, dy, dz):
+def smooth_gradients(fields, s, spacing):
+    """The smoothing MCmatlab applies to the Sobel gradients (smoothn.m with a given smoothness s,
+    no weights, no robust iterations): penalised least squares with a second-difference
+    penalty, solved in the DCT-II basis (Garcia, Comput. Stat. Data Anal. 54, 2010):
+        z = IDCT(Gamma * DCT(y)),  Gamma = 1 / (1 + s * Lambda^2),
+        Lambda = sum_i (2 - 2 cos(pi k_i / n_i)) / h_i^2,  h = spacing / max(spacing).
+    Every field is smoothed with the same s."""
+    from scipy.fft import dctn, idctn
+    shape = np.shape(fields[0])
+    h = np.asarray(spacing, dtype=np.float64)
+    h = h / h.max()
+    lam = np.zeros(shape)
+    for ax, n in enumerate(shape):
+        k = np.arange(n).reshape([n if a == ax else 1 for a in range(len(shape))])
+        lam = lam + (2.0 - 2.0 * np.cos(np.pi * k / n)) / h[ax] ** 2
+    gamma = 1.0 / (1.0 + s * lam ** 2)
+    return [idctn(gamma * dctn(np.asarray(f, dtype=np.float64), type=2, norm="ortho"), type=2, norm="ortho")
+            for f in fields]
+
+
+def interface_normals(M1, n_per_submedium, dx, dy, dz, smoothingLengthScale=0.0):
     """(theta, phi) of the interface normal per voxel, float32 [2, L] (getOpticalMediaProperties.m:222-240).
 
     M1 is the 1-based sub-medium grid; n_per_submedium is the [nSM, nL] refractive
     index table. Voxels are grouped by unique refractive-index rows; for each group the
-    Sobel gradient of the group's indicator gives the normal inside that group.
+    Sobel gradient of the group's indicator gives the normal inside that group, smoothed
+    with s = max(1, round(smoothingLengthScale / max(dx, dy, dz))) when the length scale is
+    positive (:230-231).
     """
     nrows = np.asarray(n_per_submedium, dtype=np.float64)
     if nrows.ndim == 1:
@@ -129,9 +151,13 @@ def interface_normals(M1, n_per_submedium, dx, dy, dz):
     for k in range(uniq.shape[0]):
         mask = ri_class == k
         gx, gy, gz = sobel_gradients(mask)
-        Gx[mask] = (gx / dx)[mask]
-        Gy[mask] = (gy / dy)[mask]
-        Gz[mask] = (gz / dz)[mask]
+        gx, gy, gz = gx / dx, gy / dy, gz / dz
+        if smoothingLengthScale > 0:
+            s = max(1, int(np.round(smoothingLengthScale / max(dx, dy, dz))))
+            gx, gy, gz = smooth_gradients([gx, gy, gz], s, [dx, dy, dz])
+        Gx[mask] = gx[mask]
+        Gy[mask] = gy[mask]
+        Gz[mask] = gz[mask]
     # cart2sph: phi = atan2(y, x), elevation = atan2(z, hypot(x, y)); theta = pi/2 - elevation
     phi = np.arctan2(Gy, Gx)
     elev = np.arctan2(Gz, np.hypot(Gx, Gy))
@@ -152,7 +178,7 @@ def custom_phase_cdf(phase_func, wavelength):
     return np.concatenate([[0.0], np.cumsum(pdf) / np.sum(pdf)])
 
 
-def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC):
+def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0):
     """Per-sub-medium optical tables and the sub-medium grid (getOpticalMediaProperties.m).
 
     Media with FR/T/FD-dependent properties (nBins > 1, sub-media splitting) are not
@@ -221,7 +247,7 @@ def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, d
     if np.any(np.isnan(n)) or np.any(n < 1):
         raise ValueError("Error: A medium has invalid n. Must not be NaN, must be real and at least 1.")
     M = np.asfortranarray(M_trim.astype(np.uint8))
-    normals = None if matchedInterfaces else interface_normals(M, n, dx, dy, dz)
+    normals = None if matchedInterfaces else interface_normals(M, n, dx, dy, dz, smoothingLengthScale)
     CDFs = np.stack(cdfs, axis=1) if cdfs else np.zeros((0, 0))
     return dict(mua=mua, mus=mus, g=g, n=n, CDFidx=CDFidx, M=M, CDFs=CDFs,
                 interfaceNormals=normals, minSubmediaIdx=minSub, maxSubmediaIdx=maxSub,
