@@ -72,6 +72,15 @@ struct Inst {
 
 constexpr int kGradMedia = 10;  // media supported by gradient runs
 
+// A packet ends (as killed) after this many propagation sub-steps without a scattering event.
+// The reference has no such limit: a packet that totally reflects into air voxels keeps the
+// tissue's refractive index there, meets an index mismatch at every further voxel boundary and
+// can reflect indefinitely without scattering or losing weight (seen with smoothed interface
+// normals: ~1 us per sub-step, 10 s for one packet). Between two scattering events an ordinary
+// packet crosses at most a few grid diagonals (about 3e3 voxel boundaries per diagonal of a
+// 1000^3 grid).
+constexpr uint32_t kMaxFreeSteps = 20000u;
+
 // d/dmua of c(mua) = w (1 - exp(-mua s)) / mua is w s^2 phi(mua s) with
 // phi(x) = (exp(-x) - (1 - exp(-x)) / x) / x; its Taylor series -1/2 + x/3 - x^2/8 + x^3/30
 // replaces the cancelling direct form for small x (air has mua = 1e-8 /cm)
@@ -92,6 +101,7 @@ struct Photon {
   int med;   // medium of the current voxel
   bool inbox;  // current voxel inside the gradient target box
   uint32_t scat, refr, refl, itr;
+  uint32_t nsteps;  // propagation sub-steps since launch or the last scattering event
   int kec;  // 0 killed, 1 escaped, 2 collected
   // RNG
   uint32_t pidlo, pidhi;
@@ -235,6 +245,7 @@ __device__ __forceinline__ bool launch_packet(Photon &P, const Inst &I) {
   P.sameVoxel = false;
   P.weight = 1.f;
   P.kec = 0;
+  P.nsteps = 0;
   int attempts = 0;
   float tgt[3] = {0.f, 0.f, 0.f}, w0[3];
   const float hk = kKillRange / 2.0f;
@@ -632,6 +643,7 @@ __device__ __forceinline__ bool check_escape(Photon &P, const Inst &I, bool tall
 
 // scatterPhoton (MCmatlablib.c:1138-1184)
 __device__ __forceinline__ void scatter(Photon &P, const Inst &I) {
+  P.nsteps = 0;
   float ct;
   if (isnan(P.g)) {
     const float a = rnd(P, I);

@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
             if (GRAD) P.inbox = in_box(*I, P.i);
           }
         }
+        if (++P.nsteps >= kMaxFreeSteps) P.alive = false;
       }
       if (P.alive && !(P.stepLeft > 0)) {
         if (P.weight < kThreshold) {
@@ -395,6 +396,7 @@ __global__ void example_paths_kernel(const Inst *inst, int nPaths, unsigned long
           if (tele && (I.eol || criteria_met(P, I))) path_update(W, P, I, true);
           if (P.alive) voxel_props(P, I);
         }
+        if (++P.nsteps >= kMaxFreeSteps) P.alive = false;
       }
       if (P.alive && P.weight < kThreshold) {
         if (rnd(P, I) <= kChance) P.weight /= kChance;

@@ -26,8 +26,9 @@ def _distr(v):
     return np.atleast_1d(np.asarray(v, dtype=np.float64)).reshape(1, -1)
 
 
-def prepare_mc(mdl, simType=1):
-    """Flat MEX-level inputs for one MC run (runMonteCarlo.m + getOpticalMediaProperties.m)."""
+def prepare_mc(mdl, simType=1, normals=None):
+    """Flat MEX-level inputs for one MC run (runMonteCarlo.m + getOpticalMediaProperties.m).
+    `normals` replaces prep.interface_normals (runMonteCarlo passes the device version)."""
     if simType != 1:
         raise NotImplementedError("fluorescence MC (simType 2) is not supported by this host mirror")
     G = mdl.G
@@ -50,7 +51,7 @@ def prepare_mc(mdl, simType=1):
         raise ValueError("Error: If boundaryType == 0, no photons can escape to be registered on the light collector. Disable light collector or change boundaryType.")
     media = G.mediaPropertiesFunc(G.mediaPropParams)
     mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC,
-                                       MC.smoothingLengthScale)
+                                       MC.smoothingLengthScale, normals)
     SD = MC.sourceDistribution
     if np.ndim(SD) == 0:
         sd = None

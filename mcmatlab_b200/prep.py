@@ -178,7 +178,8 @@ def custom_phase_cdf(phase_func, wavelength):
     return np.concatenate([[0.0], np.cumsum(pdf) / np.sum(pdf)])
 
 
-def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0):
+def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0,
+                             normals=None):
     """Per-sub-medium optical tables and the sub-medium grid (getOpticalMediaProperties.m).
 
     Media with FR/T/FD-dependent properties (nBins > 1, sub-media splitting) are not
@@ -247,7 +248,8 @@ def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, d
     if np.any(np.isnan(n)) or np.any(n < 1):
         raise ValueError("Error: A medium has invalid n. Must not be NaN, must be real and at least 1.")
     M = np.asfortranarray(M_trim.astype(np.uint8))
-    normals = None if matchedInterfaces else interface_normals(M, n, dx, dy, dz, smoothingLengthScale)
+    # `normals` may supply another implementation of interface_normals (the device one)
+    normals = None if matchedInterfaces else (normals or interface_normals)(M, n, dx, dy, dz, smoothingLengthScale)
     CDFs = np.stack(cdfs, axis=1) if cdfs else np.zeros((0, 0))
     return dict(mua=mua, mus=mus, g=g, n=n, CDFidx=CDFidx, M=M, CDFs=CDFs,
                 interfaceNormals=normals, minSubmediaIdx=minSub, maxSubmediaIdx=maxSub,

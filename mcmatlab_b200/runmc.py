@@ -24,7 +24,8 @@ def runMonteCarlo(model, *args):
     if model.MC.FRdepIterations:
         raise NotImplementedError("fluence-rate-dependent iterations are not part of this library")
     model.G.updateGeometry()
-    mc_in = mexargs.prepare_mc(model, 1)
+    dev = model.MC.GPUdevice
+    mc_in = mexargs.prepare_mc(model, 1, normals=lambda *a: native.interface_normals(*a, device=dev))
     out = native.mc_run(mc_in, device=model.MC.GPUdevice)
     MC = model.MC
     nL = np.asarray(mc_in["mua"]).shape[1]

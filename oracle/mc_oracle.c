@@ -108,6 +108,7 @@ typedef struct {
   unsigned long scat, refr, refl, itr;
   int kec; /* 0 killed, 1 escaped, 2 collected */
   unsigned long long steps;
+  unsigned long psteps; /* sub-steps since launch or the last scattering event */
   double L[10], k[10]; /* path length and scattering count per medium (gradient runs) */
   int inbox;
 } orc_photon;
@@ -669,11 +670,17 @@ static void scatter(orc_mc *R, orc_photon *P) {
   if ((unsigned long)m >= R->minIdx && (unsigned long)m <= R->maxIdx) P->scat++;
 }
 
+/* sub-steps without a scattering event after which a packet ends as killed: the transport's
+ * guard against packets caught in endless reflections in non-scattering regions (the reference
+ * has no limit) */
+#define ORC_MAX_FREE_STEPS 20000UL
+
 static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
   P->pid = pid;
   P->draw = 0;
   P->bufblock = 0xFFFFFFFFu;
   launch(R, P);
+  P->psteps = 0;
   for (int m = 0; m < 10; m++) P->L[m] = P->k[m] = 0.0;
   if (P->alive) {
     voxel_props(R, P);
@@ -687,12 +694,16 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
         check_escape(R, P);
         if (P->alive) voxel_props(R, P);
       }
+      if (++P->psteps >= ORC_MAX_FREE_STEPS) P->alive = false;
     }
     if (P->alive && P->weight < O_THRESHOLD) {
       if (rnd(R, P) <= O_CHANCE) P->weight /= O_CHANCE;
       else P->alive = false;
     }
-    if (P->alive) scatter(R, P);
+    if (P->alive) {
+      P->psteps = 0;
+      scatter(R, P);
+    }
   }
   if (R->eol && criteria(R, P) && R->NFR)
     for (long k = 0; k < P->recN; k++) add(&R->NFR[P->jrec[k]], P->weight * P->wrec[k]);
