@@ -306,12 +306,13 @@ __global__ void __launch_bounds__(256, 3) pass_yz_kernel(HeatDev h) {
         const float tnew = rhs[r * P + cx];
         if (ZPASS) {
           const int m = Ms[r * TW + cx];
-          if (h.dOmega && h.E[m] != 0.0) {
-            // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602),
-            // exponent evaluated in FP64 (logA ~ 154 cancels against E/RT)
-            const double tmid = 0.5 * ((double)tnew + (double)h.T[v]) + h.base + kCelsiusZero;
-            const double rate = exp(h.logA[m] - h.E[m] / (kGasR * tmid));
-            h.dOmega[v] += (float)(h.dtd * rate);
+          const float2 dg = h.dmg[m];
+          if (h.dOmega && dg.y > 0.f) {
+            // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602):
+            // log A - E / (R (T0 + d)) = x0 + (E/R) d / (T0 (T0 + d)) with x0 = log A - E / (R T0)
+            // formed in FP64 per call, so the large cancelling terms (log A ~ 154) never meet in FP32
+            const float d = 0.5f * (tnew + h.T[v]);
+            h.dOmega[v] += h.dt * expf(dg.x + dg.y * d / (h.T0 * (h.T0 + d)));
           }
           // running per-medium maximum, flushed when this thread's medium changes
           const unsigned int enc = enc_max((float)((double)tnew + h.base));
@@ -431,6 +432,9 @@ mcb_status check_params(mcb_ctx *ctx, const mcb_heat_params *p) {
   }
   for (int m = 0; m < p->nM; m++)
     if (!(p->A[m] >= 0) || !(p->E[m] >= 0)) return set_error(ctx, MCB_EINVAL, "A and E must be non-negative");
+  // every kernel indexes the media tables with M: reject indices beyond them
+  for (long long k = 0; k < L; k++)
+    if (p->M[k] >= p->nM) return set_error(ctx, MCB_EINVAL, "M holds a medium index outside 0..nM-1 (voxel %lld)", k);
   if (std::min(yz_tile_width((int)ny), yz_tile_width((int)nz)) == 0)
     return set_error(ctx, MCB_EINVAL, "y or z lines longer than the shared-memory tile limit");
   if (x_lines((int)nx) == 0) return set_error(ctx, MCB_EINVAL, "x lines longer than the shared-memory limit");
@@ -457,7 +461,7 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   const int nM = p->nM;
   const size_t need = 4 * L * 3 /*T A Q*/ + 4 * (size_t)std::max<long long>(L, nM) /*stage*/ + 12 * L /*ib*/ +
                       24 * L /*fb*/ + L /*nb*/ + 4 * L /*Sz*/ + (damage ? 8 * L : 0) + L + 12 * (size_t)nM * nM +
-                      16 * (size_t)nM + 4 * (size_t)nM + 64 + 24 * 256;
+                      24 * (size_t)nM /*logA E dmg*/ + 4 * (size_t)nM + 64 + 25 * 256;
   free_state_buffers(s);
   MCB_CUDA(ctx, cudaMalloc(&s->block, need));
   char *cur = (char *)s->block;
@@ -480,6 +484,7 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   s->c = (float *)take(12 * (size_t)nM * nM);
   s->logA = (double *)take(8 * (size_t)nM);
   s->E = (double *)take(8 * (size_t)nM);
+  s->dmg = (float2 *)take(8 * (size_t)nM);
   s->maxEnc = (unsigned int *)take(4 * (size_t)nM);
   s->step = (int *)take(16);
   s->nx = p->nx;
@@ -492,6 +497,16 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   return MCB_OK;
 }
 
+// Per medium {x0, E/R} with x0 = log A - E / (R T0), T0 = base temperature in kelvin (FP64 on the
+// host); E/R = 0 marks media without damage.
+void damage_table(const mcb_heat_params *p, double base, float2 *out) {
+  const double T0 = base + kCelsiusZero;
+  for (int m = 0; m < p->nM; m++) {
+    const double c1 = p->E[m] / kGasR;
+    out[m] = p->E[m] != 0.0 ? make_float2((float)(std::log(p->A[m]) - c1 / T0), (float)c1) : make_float2(0.f, 0.f);
+  }
+}
+
 // Uploads the media/coefficients/source of p and the state T, Omega (host pointers).
 mcb_status state_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T, const float *Omega) {
   cudaStream_t st = ctx->stream;
@@ -502,6 +517,8 @@ mcb_status state_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *
   s->base = sum / (double)L;
   std::vector<double> logA(nM);
   for (int m = 0; m < nM; m++) logA[m] = std::log(p->A[m]);
+  std::vector<float2> dmg(nM);
+  damage_table(p, s->base, dmg.data());
   MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, T, 4 * L, cudaMemcpyHostToDevice, st));
   to_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->stage, s->T, s->base, L);
   MCB_CUDA(ctx, cudaMemcpyAsync(s->M, p->M, L, cudaMemcpyHostToDevice, st));
@@ -510,7 +527,8 @@ mcb_status state_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *
   MCB_CUDA(ctx, cudaMemcpyAsync(s->c, p->dTdtperdeltaT, 12 * (size_t)nM * nM, cudaMemcpyHostToDevice, st));
   MCB_CUDA(ctx, cudaMemcpyAsync(s->logA, logA.data(), 8 * nM, cudaMemcpyHostToDevice, st));
   MCB_CUDA(ctx, cudaMemcpyAsync(s->E, p->E, 8 * nM, cudaMemcpyHostToDevice, st));
-  MCB_CUDA(ctx, cudaStreamSynchronize(st));  // host buffers (logA) go out of scope
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->dmg, dmg.data(), 8 * nM, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaStreamSynchronize(st));  // host buffers (logA, dmg) go out of scope
   s->factoredDt = -1.0;
   return MCB_OK;
 }
@@ -521,6 +539,7 @@ HeatDev make_dev(const mcb_heat_state *s, const mcb_heat_params *p) {
   h.T = s->T; h.A = s->A; h.M = s->M; h.c = s->c;
   h.Q = p->lightsOn ? s->Q : nullptr;
   h.ib = s->ib; h.fb = s->fb; h.nb = s->nb; h.Sz = s->Sz; h.Omega = s->Om; h.dOmega = s->dOm; h.logA = s->logA; h.E = s->E;
+  h.dmg = s->dmg; h.T0 = (float)(s->base + kCelsiusZero);
   h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0;
   h.dt = (float)p->dt; h.hdt = (float)(p->dt / 2); h.dtd = p->dt; h.base = s->base;
   h.nS = p->nSensors; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = s->sens; h.stepCounter = s->step;
@@ -806,6 +825,7 @@ void carve_static_state(ScratchCarve &c, mcb_heat_state *s, const mcb_heat_param
   s->M = (uint8_t *)c.take(L);
   s->c = (float *)c.take(12 * (size_t)nM * nM);
   s->logA = (double *)c.take(8 * (size_t)nM);
+  s->dmg = (float2 *)c.take(8 * (size_t)nM);
   s->E = (double *)c.take(8 * (size_t)nM);
   s->maxEnc = (unsigned int *)c.take(4 * (size_t)nM);
   s->step = (int *)c.take(16);
@@ -855,6 +875,8 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
   s.base = sum / (double)L;
   double logA[256];
   for (int m = 0; m < nM; m++) logA[m] = std::log(p->A[m]);
+  float2 dmg[256];
+  damage_table(p, s.base, dmg);
   MCB_CUDA(ctx, cudaMemcpyAsync(s.stage, T, 4 * L, cudaMemcpyHostToDevice, st));
   to_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s.stage, s.T, s.base, L);
   MCB_CUDA(ctx, cudaMemcpyAsync(s.M, p->M, L, cudaMemcpyHostToDevice, st));
@@ -863,6 +885,7 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
   MCB_CUDA(ctx, cudaMemcpyAsync(s.c, p->dTdtperdeltaT, 12 * (size_t)nM * nM, cudaMemcpyHostToDevice, st));
   MCB_CUDA(ctx, cudaMemcpyAsync(s.logA, logA, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
   MCB_CUDA(ctx, cudaMemcpyAsync(s.E, p->E, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s.dmg, dmg, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
   if (nS) {
     MCB_CUDA(ctx, cudaMemcpyAsync(s.sIdx, p->tempSensorCornerIdxs, 8 * (size_t)nS, cudaMemcpyHostToDevice, st));
     MCB_CUDA(ctx, cudaMemcpyAsync(s.sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, st));

@@ -25,6 +25,8 @@ struct HeatDev {
   float *Omega;    // or nullptr
   float *dOmega;   // damage accumulated during the current call, or nullptr
   const double *logA, *E;  // [nM]
+  const float2 *dmg;       // [nM] Arrhenius exponent about the base temperature (damage_table)
+  float T0;                // base temperature in kelvin
   unsigned int *maxEnc;    // [nM] order-preserving encoded running maxima
   int hs;          // heat-sinked faces
   float dt, hdt;

@@ -20,6 +20,7 @@ struct mcb_heat_state {
   uint8_t *nb = nullptr;
   uint8_t *M = nullptr;
   double *logA = nullptr, *E = nullptr;
+  float2 *dmg = nullptr;
   unsigned int *maxEnc = nullptr;
   int *step = nullptr;
   double *sIdx = nullptr, *sW = nullptr, *sens = nullptr;
