@@ -52,7 +52,9 @@ MCB_API mcb_status mcb_ctx_create(int device, mcb_ctx **out);
 MCB_API mcb_status mcb_ctx_destroy(mcb_ctx *ctx);
 MCB_API const char *mcb_last_error(const mcb_ctx *ctx);
 /* Host-visible cancel flag polled by the transport kernel (stands in for utIsInterruptPending,
- * MCmatlab.c:293-298). Setting *flag != 0 makes the running mcb_mc_run return MCB_ECANCELLED. */
+ * MCmatlab.c:293-298). Setting *flag != 0 makes the running mcb_mc_run return MCB_ECANCELLED;
+ * its outputs then hold the results of the packets that ran, normalised over them, as the
+ * reference returns them on Ctrl+C. The caller resets the flag. */
 MCB_API volatile int *mcb_cancel_flag(mcb_ctx *ctx);
 
 /* ------------------------------------------------------------------------------------------

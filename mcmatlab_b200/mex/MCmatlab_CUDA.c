@@ -9,18 +9,59 @@
  * mexErrMsgIdAndTxt("MCmatlab:CUDA", ...).
  *
  * Build in MATLAB (Linux):
- *   mex -I<repo>/include MCmatlab_CUDA.c -L<repo>/mcmatlab_b200 -lmcb200
+ *   mex -I<repo>/include MCmatlab_CUDA.c -L<repo>/mcmatlab_b200 -lmcb200 -lut
  * The RNG seed is the optional MC.seed property; without it the seed is taken from the
  * clock, as the reference seeds its generator (MCmatlab.c:241).
+ *
+ * Ctrl+C: the transport runs on a worker thread while the MATLAB thread polls
+ * utIsInterruptPending (as MCmatlab.c:293-298, :690-693 do) and raises the library's cancel
+ * flag; the run then stops and returns the results of the packets that ran, normalised over
+ * them, as the reference does.
  */
 #include "mex.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <stdbool.h>
 #include <stdint.h>
 #include <string.h>
 #include <time.h>
 
 #include "mcb200.h"
+
+extern bool utIsInterruptPending(void); /* libut (MATLAB) */
+
+struct run_job {
+  mcb_ctx *ctx;
+  const mcb_mc_model *m;
+  mcb_mc_result *r;
+  mcb_status st;
+  int done;
+};
+
+static void *run_worker(void *arg) {
+  struct run_job *j = (struct run_job *)arg;
+  j->st = mcb_mc_run(j->ctx, j->m, j->r);
+  __atomic_store_n(&j->done, 1, __ATOMIC_RELEASE);
+  return NULL;
+}
+
+/* mcb_mc_run on a worker thread; this (MATLAB's) thread forwards Ctrl+C to the cancel flag. */
+static mcb_status run_interruptible(mcb_ctx *ctx, const mcb_mc_model *m, mcb_mc_result *r) {
+  volatile int *cancel = mcb_cancel_flag(ctx);
+  struct run_job job = {ctx, m, r, MCB_OK, 0};
+  pthread_t th;
+  *cancel = 0;
+  if (pthread_create(&th, NULL, run_worker, &job) != 0) return mcb_mc_run(ctx, m, r);
+  const struct timespec tick = {0, 20000000}; /* 20 ms */
+  while (!__atomic_load_n(&job.done, __ATOMIC_ACQUIRE)) {
+    if (!*cancel && utIsInterruptPending()) *cancel = 1;
+    nanosleep(&tick, NULL);
+  }
+  pthread_join(th, NULL);
+  *cancel = 0;
+  return job.st;
+}
 
 static mcb_ctx *g_ctx = NULL;
 static int g_dev = -1;
@@ -202,8 +243,9 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
     g_dev = dev;
     mexAtExit(cleanup);
   }
-  const mcb_status st = mcb_mc_run(g_ctx, &m, &r);
-  if (st != MCB_OK && st != MCB_ELAUNCH) {
+  const mcb_status st = run_interruptible(g_ctx, &m, &r);
+  if (st == MCB_ECANCELLED) mexPrintf("\nCtrl+C detected, stopping.");
+  if (st != MCB_OK && st != MCB_ELAUNCH && st != MCB_ECANCELLED) {
     if (paths) mxFree(paths);
     mexErrMsgIdAndTxt("MCmatlab:CUDA", "%s", mcb_last_error(g_ctx));
   }

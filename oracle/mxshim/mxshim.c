@@ -258,7 +258,8 @@ MXS_EXPORT void mexErrMsgIdAndTxt(const char *id, const char *fmt, ...) {
 }
 MXS_EXPORT void mexErrMsgTxt(const char *msg) { fail("MEX", msg); }
 
-MXS_EXPORT bool utIsInterruptPending(void) { return false; }
+MXS_EXPORT int mxshim_interrupt = 0; /* what utIsInterruptPending reports (a test sets it) */
+MXS_EXPORT bool utIsInterruptPending(void) { return __atomic_load_n(&mxshim_interrupt, __ATOMIC_ACQUIRE) != 0; }
 
 MXS_EXPORT void *mxMalloc(size_t n) { return malloc(n ? n : 1); }
 MXS_EXPORT void *mxCalloc(size_t n, size_t size) { return calloc(n ? n : 1, size ? size : 1); }

@@ -51,3 +51,24 @@ def test_heat_gateway_matches_reference(gateways):
     np.testing.assert_allclose(S, gold["insulated_on_sensorTemps"], rtol=1e-6 * nt + 2e-6)
     np.testing.assert_allclose(Mx.ravel(), gold["insulated_on_maxMediaTemps"].ravel(), rtol=1e-6 * nt + 2e-6)
     assert S.shape == (3, nt + 1) and Mx.shape == (1, 4)
+
+
+def test_mc_gateway_ctrl_c_returns_partial_results(gateways):
+    """With MATLAB's interrupt flag raised, the gateway stops the run and returns the packets
+    that ran, normalised over them, without an error (the reference's Ctrl+C behaviour)."""
+    import ctypes as C
+    gw, _ = gateways
+    flag = C.c_int.in_dll(gw.sh.lib, "mxshim_interrupt")
+    mc_in = mexargs.prepare_mc(mccases.c0_small())
+    tree = mexargs.mex_model_tree(dict(mc_in, nPhotonsRequested=2e9, seed=3))
+    flag.value = 1
+    try:
+        out = gw.run(tree)
+    finally:
+        flag.value = 0
+    n = float(np.asarray(out["nPhotons"]).ravel()[0])
+    assert 0 < n < 2e9
+    assert np.all(np.isfinite(out["NFR"])) and float(np.max(out["NFR"])) > 0
+    # the next call runs to completion
+    out = gw.run(mexargs.mex_model_tree(dict(mc_in, seed=4)))
+    assert float(np.asarray(out["nPhotons"]).ravel()[0]) == mc_in["nPhotonsRequested"]
