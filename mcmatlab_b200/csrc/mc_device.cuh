@@ -112,7 +112,7 @@ struct Photon {
 __device__ __forceinline__ float rnd(Photon &P, const Inst &I) {
   const uint32_t k = P.draw & 3u;
   if (k == 0) {
-    Philox4 o = philox4x32_10(P.draw >> 2, P.pidlo, (P.pidhi & 0xFFFFu) | I.ctr2hi, I.stream, I.key0, I.key1);
+    Philox4 o = philox_block(P.draw >> 2, P.pidlo, (P.pidhi & 0xFFFFu) | I.ctr2hi, I.stream, I.key0, I.key1);
     P.r0 = o.x;
     P.r1 = o.y;
     P.r2 = o.z;
@@ -460,10 +460,12 @@ __device__ __forceinline__ void interface_normal(const Photon &P, const Inst &I,
 // propagatePhoton without the deposit (MCmatlablib.c:1019-1091); returns the step length s.
 __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
   P.sameVoxel = true;
-  const float q = P.stepLeft / P.mus;
+  // fast division (two-ulp, a reciprocal and a multiply): q only decides the sub-step length,
+  // and the comparison s == q below uses this same q
+  const float q = __fdividef(P.stepLeft, P.mus);
   const float s = fminf(q, fminf(P.D[0], fminf(P.D[1], P.D[2])));
   P.stepLeft = s == q ? 0.f : P.stepLeft - s * P.mus;
-  P.time += s * P.RI / kC;
+  P.time += s * P.RI * (1.0f / kC);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const float io = floorf(P.i[k]);

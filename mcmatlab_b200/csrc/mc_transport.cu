@@ -94,12 +94,14 @@ __device__ __forceinline__ unsigned long long fetch_packet(const KernelArgs &a) 
 }
 
 
-// Launch bounds: 3 blocks of 256 per SM without spills. The gradient variant keeps its
-// per-packet state (path length L_m and scattering count k_m per medium) and its per-thread box
-// partial sums in dynamic shared memory, one column per thread (grad_smem_bytes), so that it
-// runs at the plain kernel's occupancy; the medium index selects the row directly.
+// Launch bounds: the plain kernel runs 4 blocks of 256 per SM at 64 registers (about 100 bytes
+// of spill stores; measured 3-9% more packets/s than 3 blocks at 80 registers without spills);
+// the gradient variant runs 3 blocks without spills (at 64 registers it ran slower). The gradient
+// variant keeps its per-packet state (path length L_m and scattering count k_m per medium) and
+// its per-thread box partial sums in dynamic shared memory, one column per thread
+// (grad_smem_bytes), so that it holds 3 blocks per SM; the medium index selects the row directly.
 template <bool GRAD>
-__global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs a) {
   // single-instance runs read the instance and its medium table from shared memory
   __shared__ Inst sInst;
   __shared__ float4 sMed[256];
@@ -123,9 +125,15 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
   }
   int nGM = 0, nGR = 0;
   // gradient state (GRAD only): radial-bin and box sums of the block, and per-thread columns
-  // (stride blockDim.x) of L_m, k_m and the thread's box partial sums [value, d/dmua, d/dmus]
+  // (stride blockDim.x) of the packet's L_m, k_m, A_m, E_m and the thread's box partial sums
+  // [value, d/dmua, d/dmus]. The box derivatives are summed per packet in deferred form: with
+  // C the packet's box tally so far, A_m = sum over its sub-steps in m of s C (C after the
+  // sub-step) and E_m = sum over its interactions in m of C, the per-sub-step terms
+  // sum_t L_m(t) c(t) and sum_t k_m(t) c(t) equal L_m C - A_m and k_m C - E_m at the packet's
+  // end, so a box sub-step costs O(1) instead of a loop over the media.
   double *sR = gradSmem, *sF = gradSmem;
-  float *sGL = nullptr, *sGK = nullptr, *sBox = nullptr;
+  float *sGL = nullptr, *sGK = nullptr, *sGA = nullptr, *sGE = nullptr, *sBox = nullptr;
+  float boxC = 0.f;
   const int tid = threadIdx.x, bd = blockDim.x;
   if (GRAD) {
     // gradient runs are single-instance (enforced by the host)
@@ -134,7 +142,9 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
     sF = sR + nGR * (1 + 2 * nGM);
     sGL = (float *)(sF + 1 + 2 * nGM);
     sGK = sGL + nGM * bd;
-    sBox = sGK + nGM * bd;
+    sGA = sGK + nGM * bd;
+    sGE = sGA + nGM * bd;
+    sBox = sGE + nGM * bd;
     for (int k = threadIdx.x; k < nGR * (1 + 2 * nGM); k += blockDim.x) sR[k] = 0.0;
     for (int k = threadIdx.x; k < 1 + 2 * nGM; k += blockDim.x) sF[k] = 0.0;
     for (int k = threadIdx.x; k < nGM; k += blockDim.x) sInvMus[k] = 1.0f / sMed[k].y;
@@ -154,32 +164,40 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
   unsigned long long steps = 0;
   unsigned long long pid = 0;
   for (;;) {
-    // 1. a finished packet: flush its deposit run, then either start its end-of-life replay
+    // 1. a finished packet: flush its deposit run, then either queue its end-of-life replay
     //    (MCmatlab.c:262-264) or mark the lane free
+    bool relaunch = false;
     if (!P.alive && started) {
       if (accj >= 0) {
         atomic_add_f64(&I->NFR[accj], acc);
         accj = -1;
         acc = 0.0;
       }
+      if (GRAD && boxC > 0.f) {
+        for (int m = 0; m < nGM; m++) {
+          const float lc = sGL[m * bd + tid] * boxC - sGA[m * bd + tid];
+          const float kc = sGK[m * bd + tid] * boxC - sGE[m * bd + tid];
+          sBox[(1 + m) * bd + tid] -= lc;
+          sBox[(1 + nGM + m) * bd + tid] += kc * sInvMus[m] - lc;
+        }
+        boxC = 0.f;
+      }
       if (I->eol && !replay && I->NFR && criteria_met(P, *I)) {
         replay = true;
         wfinal = P.weight;
-        P.pidlo = (uint32_t)pid;
-        P.pidhi = (uint32_t)(pid >> 32);
-        P.draw = 0;
-        launch_packet(P, *I);
-        voxel_props(P, *I);
+        relaunch = true;
       } else {
         replay = false;
         started = false;
       }
     }
     // 2. refill free lanes in groups
-    const unsigned freeLanes = __ballot_sync(0xffffffffu, !P.alive && !retired);
-    const unsigned liveLanes = __ballot_sync(0xffffffffu, P.alive);
+    const bool idle = !P.alive && !retired && !relaunch;
+    const unsigned freeLanes = __ballot_sync(0xffffffffu, idle);
+    const unsigned liveLanes = __ballot_sync(0xffffffffu, P.alive || relaunch);
+    bool fresh = false;
     if (freeLanes && (__popc(freeLanes) >= a.refillMin || liveLanes == 0)) {
-      if (!P.alive && !retired) {
+      if (idle) {
         const unsigned long long g = fetch_packet(a);
         if (g == ~0ull) {
           retired = true;
@@ -188,24 +206,34 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
           if (!single) I = a.insts + ii;
           pid = g - (single ? 0ull : __ldg(a.instFirst + ii));
           pid = I->pOff + I->pStride * pid;
-          P.pidlo = (uint32_t)pid;
-          P.pidhi = (uint32_t)(pid >> 32);
-          P.draw = 0;
-          if (launch_packet(P, *I)) {
-            voxel_props(P, *I);
-            atomicAdd(&I->ctr[0], 1ull);
-            started = true;
-            if (GRAD) {
-              for (int m = 0; m < nGM; m++) {
-                sGL[m * bd + tid] = 0.f;
-                sGK[m * bd + tid] = 0.f;
-              }
-              P.inbox = in_box(*I, P.i);
+          fresh = true;
+        }
+      }
+    }
+    // one call site launches new packets and replays (launchPhoton is the largest routine; two
+    // inlined copies cost instruction-cache misses)
+    if (fresh || relaunch) {
+      P.pidlo = (uint32_t)pid;
+      P.pidhi = (uint32_t)(pid >> 32);
+      P.draw = 0;
+      const bool ok = launch_packet(P, *I);
+      if (ok || relaunch) voxel_props(P, *I);
+      if (fresh) {
+        if (ok) {
+          atomicAdd(&I->ctr[0], 1ull);
+          started = true;
+          if (GRAD) {
+            for (int m = 0; m < nGM; m++) {
+              sGL[m * bd + tid] = 0.f;
+              sGK[m * bd + tid] = 0.f;
+              sGA[m * bd + tid] = 0.f;
+              sGE[m * bd + tid] = 0.f;
             }
-          } else {
-            atomicAdd(&I->ctr[3], 1ull);
-            atomicOr(a.status, 2);
+            P.inbox = in_box(*I, P.i);
           }
+        } else {
+          atomicAdd(&I->ctr[3], 1ull);
+          atomicOr(a.status, 2);
         }
       }
     }
@@ -223,22 +251,21 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
           // perturbation MC: the box tally c = absorb / mua_j (fluence-rate estimator) depends on
           // mua through the weight (-L_m c) and through the sub-step itself; on mus through the
           // score of the sampled path up to the end of this sub-step: k_m / mus_m - L_m, where
-          // k counts the interaction that ends the sub-step when the free path ran out here
+          // k counts the interaction that ends the sub-step when the free path ran out here.
+          // This sub-step's own terms are added now; the terms of the earlier path (L_m, k_m
+          // before this sub-step) are added at the packet's end in the deferred form above.
           if (P.inside && P.inbox) {
             const float mua = P.mua;
             const float c = absorb / mua;
             const float dself = wpre * s * s * self_phi(mua * s);
             const float kself = P.stepLeft > 0 ? 0.f : 1.f;
+            boxC += c;
             sBox[tid] += c;
-            for (int m = 0; m < nGM; m++) {
-              const float Lm = sGL[m * bd + tid];
-              const float Lincl = Lm + (m == mj ? s : 0.f);
-              const float kincl = sGK[m * bd + tid] + (m == mj ? kself : 0.f);
-              sBox[(1 + m) * bd + tid] += -Lm * c + (m == mj ? dself : 0.f);
-              sBox[(1 + nGM + m) * bd + tid] += (kincl * sInvMus[m] - Lincl) * c;
-            }
+            sBox[(1 + mj) * bd + tid] += dself;
+            sBox[(1 + nGM + mj) * bd + tid] += (kself * sInvMus[mj] - s) * c;
           }
           sGL[mj * bd + tid] += s;
+          if (boxC > 0.f) sGA[mj * bd + tid] += s * boxC;
         }
         if (P.inside && I->NFR) {
           double c = 0.0;
@@ -291,7 +318,10 @@ __global__ void __launch_bounds__(256, 3) transport_kernel(KernelArgs a) {
           else P.alive = false;
         }
         if (P.alive) {
-          if (GRAD) sGK[P.med * bd + tid] += 1.f;
+          if (GRAD) {
+            sGK[P.med * bd + tid] += 1.f;
+            if (boxC > 0.f) sGE[P.med * bd + tid] += boxC;
+          }
           scatter(P, *I);
         }
       }
@@ -813,7 +843,7 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
 // Dynamic shared memory of the gradient kernel: the block's radial-bin and box sums (FP64) and
 // per-thread columns of L_m, k_m and the box partial sums (FP32).
 size_t grad_smem_bytes(int nM, int nR, int threads) {
-  return 8 * (size_t)(nR * (1 + 2 * nM) + 1 + 2 * nM) + 4 * (size_t)threads * (2 * nM + 1 + 2 * nM);
+  return 8 * (size_t)(nR * (1 + 2 * nM) + 1 + 2 * nM) + 4 * (size_t)threads * (4 * nM + 1 + 2 * nM);
 }
 
 mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &insts, bool openEnded,

@@ -41,6 +41,16 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
   return Philox4{c0, c1, c2, c3};
 }
 
+#ifdef __CUDACC__
+// One out-of-line copy for the device: the transport inlines its ~60 draw sites, and a Philox
+// block inlined at each of them made the kernel large enough to stall on instruction fetch
+// (measured 5% more packets/s with this single copy).
+static __device__ __noinline__ Philox4 philox_block(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                                    uint32_t k1) {
+  return philox4x32_10(c0, c1, c2, c3, k0, k1);
+}
+#endif
+
 __host__ __device__ __forceinline__ float u01_from_word(uint32_t w) {
   return (float)((w >> 8) + 1u) * (1.0f / 16777216.0f);
 }
