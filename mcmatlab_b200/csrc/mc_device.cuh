@@ -53,6 +53,7 @@ struct Inst {
   // deposition criteria (counters saturate at UINT32_MAX = "infinity")
   uint32_t minS, maxS, minRefr, maxRefr, minRefl, maxRefl, minI, maxI, minIdx, maxIdx;
   int onlyCollected, eol;
+  int crit;  // a deposition criterion is set (criteria_met is true otherwise)
   // FP64 tallies
   double *NFR, *image, *FF, *NIxp, *NIxn, *NIyp, *NIyn, *NIzp, *NIzn;
   unsigned long long *ctr;  // [0] launched, [1] collected, [2] sub-steps, [3] failed launches
@@ -188,6 +189,7 @@ __device__ double lambert_wm1(double x) {
 }
 
 __device__ __forceinline__ bool criteria_met(const Photon &P, const Inst &I) {
+  if (!I.crit) return true;
   const bool killed = !P.alive && P.kec == 0;
   return P.scat >= I.minS && (killed ? 0xFFFFFFFFu : P.scat) <= I.maxS && P.refr >= I.minRefr &&
          (killed ? 0xFFFFFFFFu : P.refr) <= I.maxRefr && P.refl >= I.minRefl &&

@@ -810,9 +810,12 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     I.maxIdx = inf_cast(m->DC_maxSubmediaIdx) - 1;
     I.onlyCollected = m->DC_onlyCollected;
     I.eol = m->DC_evaluateOnlyAtEndOfLife;
+    I.crit = 1;
     if (I.minS == 0 && I.maxS == 0xFFFFFFFFu && I.minRefr == 0 && I.maxRefr == 0xFFFFFFFFu && I.minRefl == 0 &&
-        I.maxRefl == 0xFFFFFFFFu && I.minI == 0 && I.maxI == 0xFFFFFFFFu && !I.onlyCollected)
+        I.maxRefl == 0xFFFFFFFFu && I.minI == 0 && I.maxI == 0xFFFFFFFFu && !I.onlyCollected) {
       I.eol = 0;  // MCmatlab.c:418-424
+      I.crit = 0;
+    }
     I.NFR = pl.accNFR ? pl.accNFR + (size_t)iL * L : nullptr;
     I.image = pl.accImg ? pl.accImg + (size_t)iL * pl.Lim : nullptr;
     I.FF = pl.accFF ? pl.accFF + (size_t)iL * pl.Lff : nullptr;
