@@ -162,7 +162,7 @@ def interface_normals(M1, n_per_submedium, dx, dy, dz, smoothingLengthScale=0.0)
     phi = np.arctan2(Gy, Gx)
     elev = np.arctan2(Gz, np.hypot(Gx, Gy))
     theta = np.pi / 2 - elev
-    out = np.empty((2, M1.size), dtype=np.float32)
+    out = np.empty((2, M1.size), dtype=np.float32, order="F")  # MATLAB order: (theta, phi) per voxel
     out[0] = theta.reshape(-1, order="F")
     out[1] = phi.reshape(-1, order="F")
     return out
