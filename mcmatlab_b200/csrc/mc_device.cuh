@@ -525,6 +525,15 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
 
 __device__ __forceinline__ void atomic_add_f64(double *p, double v) { atomicAdd(p, v); }
 
+// Absorbed fraction 1 - exp(-x), x = mua s >= 0 (MCmatlablib.c evaluates -expm1(-mua s)):
+// the Taylor series below x = 1/16 (truncation below 2e-9 relative), 1 - expf(-x) above, where
+// the subtraction loses at most a factor 16 of expf's relative error
+__device__ __forceinline__ float one_minus_exp_neg(float x) {
+  if (x < 0.0625f)
+    return x * (1.f - x * (0.5f - x * (1.f / 6.f - x * (1.f / 24.f - x * (1.f / 120.f - x * (1.f / 720.f))))));
+  return 1.f - expf(-x);
+}
+
 // formImage (MCmatlablib.c:737-788)
 // With tally == false only the classification (P.kec) is updated.
 __device__ __forceinline__ void form_image(Photon &P, const Inst &I, bool tally) {

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
         const float wpre = GRAD ? P.weight : 0.f;
         const float s = propagate(P, *I);
         steps++;
-        const float absorb = -P.weight * expm1f(-P.mua * s);
+        const float absorb = P.weight * one_minus_exp_neg(P.mua * s);
         P.weight -= absorb;
         if (GRAD) {
           // perturbation MC: the box tally c = absorb / mua_j (fluence-rate estimator) depends on
@@ -418,7 +418,7 @@ __global__ void example_paths_kernel(const Inst *inst, int nPaths, unsigned long
     while (P.alive) {
       while (P.alive && P.stepLeft > 0) {
         const float s = propagate(P, I);
-        const float absorb = -P.weight * expm1f(-P.mua * s);
+        const float absorb = P.weight * one_minus_exp_neg(P.mua * s);
         P.weight -= absorb;
         path_update(W, P, I, false);
         if (!P.sameVoxel) {
