@@ -26,18 +26,38 @@ def _distr(v):
     return np.atleast_1d(np.asarray(v, dtype=np.float64)).reshape(1, -1)
 
 
+_RESTRICTIVE = ("minScatterings", "maxScatterings", "minRefractions", "maxRefractions", "minReflections",
+                "maxReflections", "minInterfaceTransitions", "maxInterfaceTransitions")
+
+
 def prepare_mc(mdl, simType=1, normals=None):
     """Flat MEX-level inputs for one MC run (runMonteCarlo.m + getOpticalMediaProperties.m).
-    `normals` replaces prep.interface_normals (runMonteCarlo passes the device version)."""
-    if simType != 1:
-        raise NotImplementedError("fluorescence MC (simType 2) is not supported by this host mirror")
+
+    simType 1 reads model.MC; simType 2 (fluorescence) reads model.FMC, as MCmatlab.c:322-323
+    does, and builds the fluorescence source from the excitation run's model.MC results
+    (runMonteCarlo.m:119-166, prep.fluorescence_source), which it also stores in
+    model.FMC.sourceDistribution. `normals` replaces prep.interface_normals (runMonteCarlo
+    passes the device version)."""
+    if simType not in (1, 2):
+        raise ValueError("simType must be 1 (MC) or 2 (fluorescence MC)")
     G = mdl.G
-    MC = mdl.MC
+    MC = mdl.FMC if simType == 2 else mdl.MC
     if G.M_raw is None:
         G.updateGeometry()
     wl = np.atleast_1d(np.asarray(MC.wavelength, dtype=np.float64))
-    spectrum = np.array([float(MC.spectrumFunc(w)) for w in wl])
-    spectrum = spectrum / spectrum.sum()
+    if np.any(np.isnan(wl)):
+        raise ValueError("Error: No wavelength defined")
+    if simType == 1:
+        spectrum = np.array([float(MC.spectrumFunc(w)) for w in wl])
+        spectrum = spectrum / spectrum.sum()
+    else:
+        spectrum = np.ones(wl.size)  # not read by the MEX when a source distribution is given
+        if np.size(mdl.MC.NFR) <= 1:
+            raise ValueError("Error: normalizedFluenceRate matrix not calculated for excitation light")
+        eDC = mdl.MC.depositionCriteria
+        if (any(getattr(eDC, k) != (0 if k.startswith("min") else math.inf) for k in _RESTRICTIVE)
+                or eDC.onlyCollected):
+            raise ValueError("The excitation step must be calculated without restrictive deposition criteria in order to calculate fluorescence.")
     DC = MC.depositionCriteria
     if DC.onlyCollected and not DC.evaluateOnlyAtEndOfLife:
         raise ValueError("Error: depositionCriteria.onlyCollected = true requires depositionCriteria.evaluateOnlyAtEndOfLife = true.")
@@ -52,6 +72,12 @@ def prepare_mc(mdl, simType=1, normals=None):
     media = G.mediaPropertiesFunc(G.mediaPropParams)
     mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC,
                                        MC.smoothingLengthScale, normals)
+    if simType == 2:
+        T = np.broadcast_to(np.asarray(mdl.HS.T, dtype=np.float32), G.M_raw.shape)
+        FD = (1 - np.exp(-np.asarray(mdl.HS.Omega, dtype=np.float64))).astype(np.float32)
+        NFR = np.asarray(mdl.MC.NFR, dtype=np.float32)
+        FR = (mdl.MC.P * (NFR.sum(axis=3) if NFR.ndim == 4 else NFR)).astype(np.float32)
+        MC.sourceDistribution = prep.fluorescence_source(media, G.M_raw, mdl.MC.NA, mdl.MC.wavelength, wl, FR, T, FD)
     SD = MC.sourceDistribution
     if np.ndim(SD) == 0:
         sd = None
@@ -63,8 +89,10 @@ def prepare_mc(mdl, simType=1, normals=None):
             raise ValueError("Error: model.MC.sourceDistribution must be of size [nx, ny, nz, nLambda]")
         if np.any(~np.isfinite(sd)) or np.any(sd < 0):
             raise ValueError("Error: model.MC.sourceDistribution must be real, finite and non-negative")
-        # runMonteCarlo.m:65 normalises the distributed source to unit integral
-        sd = (sd / (G.dx * G.dy * G.dz * sd.sum(dtype=np.float64))).astype(np.float32)
+        if simType == 1:
+            # runMonteCarlo.m:65 normalises the excitation source to unit integral; the
+            # fluorescence source keeps its scale (each wavelength's power is its integral)
+            sd = (sd / (G.dx * G.dy * G.dz * sd.sum(dtype=np.float64))).astype(np.float32)
         sd = np.asfortranarray(sd)
     LS = MC.lightSource
     if sd is None and LS.sourceType in (3, 4, 5):
@@ -116,7 +144,7 @@ def prepare_mc(mdl, simType=1, normals=None):
                 maxInterfaceTransitions=float(DC.maxInterfaceTransitions),
                 minSubmediaIdx=float(mp["minSubmediaIdx"]), maxSubmediaIdx=float(mp["maxSubmediaIdx"]),
                 onlyCollected=bool(DC.onlyCollected), evaluateOnlyAtEndOfLife=bool(DC.evaluateOnlyAtEndOfLife)),
-        mediaNames=mp["names"],
+        mediaNames=mp["names"], simType=simType,
     )
 
 
@@ -141,6 +169,8 @@ def mex_model_tree(mc_in):
         useAllCPUs=mc_in["useAllCPUs"], GPUdevice=float(mc_in["GPUdevice"]), seed=float(mc_in["seed"]),
     )
     G = dict(dx=float(mc_in["dx"]), dy=float(mc_in["dy"]), dz=float(mc_in["dz"]))
+    if mc_in.get("simType", 1) == 2:
+        return dict(MC=dict(), G=G, FMC=MC)
     return dict(MC=MC, G=G, FMC=dict())
 
 

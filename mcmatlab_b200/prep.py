@@ -256,6 +256,73 @@ def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, d
                 names=names)
 
 
+def _eval_yield(f, wavelength, FR, T, FD):
+    """QY or ES of one medium at one wavelength over that medium's voxels: a number, f(wavelength)
+    or f(wavelength, FR, T, FD) with FR, T, FD the voxels' arrays (element-wise, as the
+    reference requires of four-argument functions, runMonteCarlo.m:135-137)."""
+    if callable(f):
+        return f(wavelength) if _nargs(f) == 1 else f(wavelength, FR, T, FD)
+    return f
+
+
+def fluorescence_source(mediaList, M_raw, NA, Ls_E, Ls_F, FR, T, FD):
+    """Fluorescence source distribution [nx, ny, nz, nL_F] float32 (runMonteCarlo.m:119-166).
+
+    NA is the excitation run's normalised absorption [nx, ny, nz, nL_E]; FR, T and FD are the
+    fluence rate, temperature and fractional damage grids the yields may depend on. Per voxel
+    the emitted photon count is sum over excitation wavelengths of NA * QY * lambda_E (absorbed
+    power / photon energy, up to a constant), spread over the fluorescence wavelengths by the
+    voxel's emission spectrum normalised to unit sum, divided by lambda_F (power per photon).
+    Media are indexed by the raw geometry (1-based positions in mediaList), as the reference
+    loops over all media of the list.
+    """
+    Ls_E = np.atleast_1d(np.asarray(Ls_E, dtype=np.float64))
+    Ls_F = np.atleast_1d(np.asarray(Ls_F, dtype=np.float64))
+    shape = np.shape(M_raw)
+    NA4 = np.asarray(NA, dtype=np.float64)
+    if NA4.ndim == 3:
+        NA4 = NA4[..., None]
+    nLE, nLF = Ls_E.size, Ls_F.size
+    if NA4.shape != tuple(shape) + (nLE,):
+        raise ValueError("Error: normalizedAbsorption must be of size [nx, ny, nz, nLambda_excitation]")
+    Mflat = np.asarray(M_raw).reshape(-1, order="F")
+    NAf = NA4.reshape(-1, nLE, order="F")
+    FRf = np.broadcast_to(np.asarray(FR, dtype=np.float32), shape).reshape(-1, order="F")
+    Tf = np.broadcast_to(np.asarray(T, dtype=np.float32), shape).reshape(-1, order="F")
+    FDf = np.broadcast_to(np.asarray(FD, dtype=np.float32), shape).reshape(-1, order="F")
+    Fphotons = np.zeros(Mflat.size)
+    emSp = np.full((Mflat.size, nLF), np.nan)
+    for iM, med in enumerate(mediaList):
+        idx = np.nonzero(Mflat == iM + 1)[0]
+        if idx.size == 0:
+            continue
+        acc = np.zeros(idx.size)
+        for iLE in range(nLE):
+            try:
+                qy = _eval_yield(med.QY, Ls_E[iLE], FRf[idx], Tf[idx], FDf[idx])
+            except Exception as e:
+                raise ValueError("Error: The QY function of medium %s is throwing an error: %s" % (med.name, e))
+            acc = acc + NAf[idx, iLE] * np.asarray(qy, dtype=np.float64) * Ls_E[iLE]
+        Fphotons[idx] = acc
+        for iLF in range(nLF):
+            try:
+                es = _eval_yield(med.ES, Ls_F[iLF], FRf[idx], Tf[idx], FDf[idx])
+            except Exception as e:
+                raise ValueError("Error: The ES function of medium %s is throwing an error: %s" % (med.name, e))
+            emSp[idx, iLF] = np.asarray(es, dtype=np.float64)
+    if np.any(~np.isfinite(Fphotons)) or np.any(Fphotons < 0):
+        raise ValueError("Error: A quantum yield function is returning values that are not finite, real and non-negative.")
+    if np.any(~np.isfinite(emSp)) or np.any(emSp < 0):
+        raise ValueError("Error: An emission spectrum function is returning values that are not finite, real and non-negative.")
+    with np.errstate(invalid="ignore", divide="ignore"):
+        emSp = emSp / emSp.sum(axis=1, keepdims=True)
+        S = Fphotons[:, None] * emSp / Ls_F[None, :]
+    S = S.astype(np.float32)  # FMC.sourceDistribution is a single-precision property
+    if not np.nanmax(S, initial=0.0) > 0:
+        raise ValueError("Error: No fluorescence emitters")
+    return np.asfortranarray(S.reshape(tuple(shape) + (nLF,), order="F"))
+
+
 def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0):
     """VHC, TC, A, E per sub-medium and the sub-medium grid (getThermalMediaProperties.m).
 

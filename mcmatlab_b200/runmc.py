@@ -3,7 +3,11 @@
 Steps (runMonteCarlo.m line numbers): geometry update (:51-52), spectrum and distributed-source
 normalisation (:59-65), input checks (:220-375) and media preparation
 (getOpticalMediaProperties) in mexargs.prepare_mc, the MEX call (:174) replaced by
-mcb_mc_run, then the light-collector and far-field axes (:198-216).
+mcb_mc_run, then the light-collector and far-field axes (:182-216).
+
+`runMonteCarlo(model, 'fluorescence')` (simType 2) runs the fluorescence step: the source is
+built from the excitation results in model.MC (:119-166) and the run's settings and results
+live in model.FMC, as in the reference.
 """
 from __future__ import annotations
 
@@ -19,17 +23,17 @@ def _squeeze_last(a, nL):
 
 
 def runMonteCarlo(model, *args):
-    if "fluorescence" in args:
-        raise NotImplementedError("fluorescence Monte Carlo is not part of this library")
-    if model.MC.FRdepIterations:
+    simType = 2 if "fluorescence" in args else 1
+    MC = model.FMC if simType == 2 else model.MC
+    if simType == 1 and model.MC.FRdepIterations:
         raise NotImplementedError("fluence-rate-dependent iterations are not part of this library")
     model.G.updateGeometry()
-    dev = model.MC.GPUdevice
-    mc_in = mexargs.prepare_mc(model, 1, normals=lambda *a: native.interface_normals(*a, device=dev))
-    out = native.mc_run(mc_in, device=model.MC.GPUdevice)
-    MC = model.MC
+    dev = MC.GPUdevice
+    mc_in = mexargs.prepare_mc(model, simType, normals=lambda *a: native.interface_normals(*a, device=dev))
+    out = native.mc_run(mc_in, device=dev)
     nL = np.asarray(mc_in["mua"]).shape[1]
-    MC.spectrum = mc_in["spectrum"]
+    if simType == 1:
+        MC.spectrum = mc_in["spectrum"]
     MC.mediaProperties = {"name": mc_in["mediaNames"], "mua": mc_in["mua"], "mus": mc_in["mus"], "g": mc_in["g"],
                           "n": mc_in["n"], "CDFidx": mc_in["CDFidx"]}
     MC.M = mc_in["M"]

@@ -145,32 +145,38 @@ class RefMC:
         self.lib = C.CDLL(os.path.join(REF_DIR, libname))
         self.fn = self.lib.mexFunction
 
-    def run(self, tree, seed=None, nthreads=None):
+    def run(self, tree, seed=None, nthreads=None, simType=None):
+        """Runs the MEX on a property tree (mexargs.mex_model_tree). simType 2 (fluorescence) makes
+        the MEX read and write the tree's FMC node (MCmatlab.c:322-323, :463); by default it
+        follows the tree (FMC when that node is filled)."""
         sh = self.sh
+        if simType is None:
+            simType = 2 if tree.get("FMC") else 1
+        key = "FMC" if simType == 2 else "MC"
         t = dict(tree)
-        t["MC"] = dict(tree["MC"])
+        t[key] = dict(tree[key])
         # outputs the MEX overwrites are created up front, as MATLAB's object would hold them
         for k in self.OUTPUTS:
-            t["MC"].setdefault(k, np.nan)
-        t["MC"]["LC"] = dict(tree["MC"]["LC"])
-        t["MC"]["LC"].setdefault("image", np.nan)
+            t[key].setdefault(k, np.nan)
+        t[key]["LC"] = dict(tree[key]["LC"])
+        t[key]["LC"].setdefault("image", np.nan)
         if seed is not None:
-            t["MC"]["useAllCPUs"] = True
+            t[key]["useAllCPUs"] = True
             sh.fixed_us.value = int(seed)
             sh.nprocs.value = 1
         else:
             sh.fixed_us.value = -1
             sh.nprocs.value = int(nthreads) if nthreads else 0
             if nthreads:
-                t["MC"]["useAllCPUs"] = True
+                t[key]["useAllCPUs"] = True
         root = sh.tree(t)
-        simtype = sh.array(1.0)
+        simtype = sh.array(float(simType))
         try:
             (out,) = sh.call(self.fn, 1, [root, simtype])
         finally:
             sh.fixed_us.value = -1
             sh.nprocs.value = 0
-        MC = sh.get(out, "MC")
+        MC = sh.get(out, key)
         res = {}
         for k in self.OUTPUTS:
             res[k] = sh.to_numpy(sh.get(MC, k))

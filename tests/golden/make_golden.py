@@ -6,6 +6,7 @@ pinned on outputs of the reference MEX sources compiled here (oracle/_ref, built
 
   mc_ref_summaries.json   K reference batches (pinned dSFMT seeds 101..) of summary
                           statistics (tests/mcstats.py) for every case in tests/mccases.py
+                          (CASES as MC runs, FLUO_CASES as fluorescence runs)
   heat_ref.npz            reference FP32 heat MEX outputs for small seeded problems
 
 Run from the repository root:  python tests/golden/make_golden.py
@@ -36,6 +37,11 @@ def main():
     for name, fn in mccases.CASES.items():
         mc_in = mexargs.prepare_mc(fn())
         tree = mexargs.mex_model_tree(mc_in)
+        out[name] = [mcstats.summaries(R.run(tree, seed=101 + s), mc_in) for s in range(K)]
+        print(name, "done", flush=True)
+    for name, fn in mccases.FLUO_CASES.items():
+        mc_in = mexargs.prepare_mc(fn(), 2)
+        tree = mexargs.mex_model_tree(mc_in)  # filled FMC node: the MEX runs as simType 2
         out[name] = [mcstats.summaries(R.run(tree, seed=101 + s), mc_in) for s in range(K)]
         print(name, "done", flush=True)
     with open(os.path.join(HERE, "mc_ref_summaries.json"), "w") as f:

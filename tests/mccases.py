@@ -203,6 +203,45 @@ def broadband():
     return m
 
 
+def _fluo_media(params):
+    return [mm.mediumProperties(name="top", mua=2.0, mus=80.0, g=0.8, n=1.0),
+            mm.mediumProperties(name="mid", mua=lambda wl: 5.0 if wl < 500 else 2.0, mus=120.0, g=0.9, n=1.37,
+                                QY=0.4, ES=lambda wl: math.exp(-((wl - 560.0) / 40.0) ** 2)),
+            mm.mediumProperties(name="bottom", mua=1.0, mus=60.0, g=0.7, n=1.4,
+                                QY=lambda wl, FR, T, FD: 0.1 * (1 + 0.01 * (T - 37.0)) + 0 * FR,
+                                ES=lambda wl, FR, T, FD: wl / 600.0 + 0 * T)]
+
+
+def fluorescence_excited(nph=2e4):
+    """A slab whose excitation step (450 nm) has a seeded synthetic fluence-rate field in place of
+    a transport run, so that the fluorescence inputs are identical wherever they are built. The
+    middle medium emits with a constant yield and a Gaussian spectrum, the bottom one with a
+    temperature-dependent yield (HS.T = 40) and a linear spectrum; the top one does not emit."""
+    from mcmatlab_b200 import mexargs
+    m = _slab(nph=nph)
+    m.G.mediaPropertiesFunc = _fluo_media
+    m.MC.wavelength = 450.0
+    m.MC.matchedInterfaces = False
+    m.HS.T = 40.0
+    ex = mexargs.prepare_mc(m, 1)
+    X, Y, Z = np.meshgrid(m.G.x, m.G.y, m.G.z, indexing="ij")
+    m.MC.M = ex["M"]
+    m.MC.mediaProperties = {"name": ex["mediaNames"], "mua": ex["mua"], "mus": ex["mus"], "g": ex["g"], "n": ex["n"],
+                            "CDFidx": ex["CDFidx"]}
+    m.MC.normalizedFluenceRate = (np.exp(-Z / 0.03) * np.exp(-(X ** 2 + Y ** 2) / 0.03 ** 2)).astype(np.float32)
+    F = m.FMC
+    F.wavelength = np.array([550.0, 650.0])
+    F.nPhotonsRequested = nph
+    F.silentMode = True
+    F.matchedInterfaces = False
+    F.boundaryType = 1
+    F.farFieldRes = 8
+    return m
+
+
+# fluorescence runs (simType 2): prepared with mexargs.prepare_mc(model, 2)
+FLUO_CASES = {"fluorescence": fluorescence_excited}
+
 CASES = {
     "c0_small": c0_small,
     "c0_matched": c0_matched,
