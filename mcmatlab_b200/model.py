@@ -310,3 +310,9 @@ class model:
     def simulateHeatDistribution(self):
         from .heatsim import simulateHeatDistribution
         return simulateHeatDistribution(self)
+
+
+def combineModels(modelArray, simType):
+    """+MCmatlab/@model/combineModels.m: one model holding the merged results of several runs."""
+    from .combine import combineModels as _combine
+    return _combine(modelArray, simType)
