@@ -59,8 +59,10 @@ def test_mex_gateway_fluorescence_matches_reference():
 
 def test_run_monte_carlo_then_fluorescence_end_to_end():
     """Excitation transport, then the fluorescence step from its results: outputs land in
-    model.FMC, and per fluorescence wavelength absorbed + escaped power equals the source's
-    power (its integral), up to roulette noise."""
+    model.FMC, and per fluorescence wavelength absorbed + escaped equals P^2, P the source's
+    integral, up to roulette noise: the reference normalises a distributed-source run by
+    nPhotons / P (MCmatlab.c:752 passes P as the power fraction) and divides once more by P
+    (MCmatlablib.c:1195-1198)."""
     m = mccases.fluorescence_excited(nph=1e5)
     m.MC.normalizedFluenceRate = 0
     m.MC.nPhotonsRequested = 1e5
@@ -84,4 +86,4 @@ def test_run_monte_carlo_then_fluorescence_end_to_end():
         P = S[..., iL].sum() * dV
         absorbed = sum(v for k, v in s.items() if k.startswith("abs_m") and k.endswith("_l%d" % iL))
         escaped = sum(v for k, v in s.items() if k.startswith("NI_") and k.endswith("_l%d" % iL))
-        assert abs((absorbed + escaped) / P - 1.0) < 0.02, (iL, absorbed, escaped, P)
+        assert abs((absorbed + escaped) / P ** 2 - 1.0) < 0.02, (iL, absorbed, escaped, P)
