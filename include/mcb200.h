@@ -260,6 +260,16 @@ MCB_API mcb_status mcb_interface_normals(mcb_ctx *ctx, int32_t nx, int32_t ny, i
                                          const int32_t *riClass, int32_t nClass, double dx, double dy, double dz,
                                          double smoothingLengthScale, float *thetaPhi);
 
+/* Sub-media binning of a medium whose optical properties depend on fluence rate, temperature
+ * or damage, on the device. Replaces the MEX getDownsampledParamVals (+MCmatlab/src/
+ * getDownsampledParamVals.c:54-202, called from getOpticalMediaProperties.m:151): paramVals
+ * [3 x n] (column-major: mua, mus, g of each of the medium's n voxels) are downsampled to nBins
+ * representatives by greedy farthest-point selection in range-normalised coordinates;
+ * downsampled [3 x nBins] receives them, binidx [n] each voxel's 1-based nearest representative.
+ * Same arithmetic and index choices as the reference build, bit for bit. nBins in 1..255. */
+MCB_API mcb_status mcb_downsample_params(mcb_ctx *ctx, const float *paramVals, int64_t n, int32_t nBins,
+                                         float *downsampled, uint8_t *binidx);
+
 /* No counterpart in the reference: measures the device's FP64 atomicAdd throughput to
  * scattered addresses of a buffer of `slots` doubles (the transport's roofline denominator:
  * one FP64 deposit per propagation sub-step). */

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmcb200.so")
-SOURCES = ["capi.cu", "mc_transport.cu", "heat_adi.cu", "heat_adjoint.cu", "normals.cu"]
+SOURCES = ["capi.cu", "mc_transport.cu", "heat_adi.cu", "heat_adjoint.cu", "normals.cu", "downsample.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-Xptxas", "-v", "--expt-relaxed-constexpr"]
@@ -39,7 +39,7 @@ def build(force=False, verbose=False):
     logs = []
     for src in SOURCES:
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-dc" if False else "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         logs.append(r.stdout + r.stderr)
         if r.returncode != 0:

@@ -76,6 +76,7 @@ enum PoolSlot {
   SLOT_HEAT_ADJ,
   SLOT_PROBE,
   SLOT_NORMALS,
+  SLOT_DOWNSAMPLE,
   SLOT_BATCH_BASE = 40
 };
 

@@ -25,7 +25,7 @@ STATUS = {0: "MCB_OK", 1: "MCB_EINVAL", 2: "MCB_ENOMEM", 3: "MCB_ECUDA", 4: "MCB
 
 EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_flag", "mcb_mc_run", "mcb_mc_run_batch",
            "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint", "mcb_probe_atomics",
-           "mcb_interface_normals",
+           "mcb_interface_normals", "mcb_downsample_params",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
            "mcb_heat_state_destroy", "mcb_last_kernel_ms")
 
@@ -71,6 +71,8 @@ def lib():
             L.mcb_interface_normals.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint8),
                                                 C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
                                                 C.c_double, C.c_double, C.POINTER(C.c_float)]
+            L.mcb_downsample_params.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int64, C.c_int32,
+                                                C.POINTER(C.c_float), C.POINTER(C.c_uint8)]
             L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
             L.mcb_last_kernel_ms.restype = C.c_double
             _lib = L
@@ -208,6 +210,23 @@ def interface_normals(M1, n_per_submedium, dx, dy, dz, smoothingLengthScale=0.0,
                                        float(dy), float(dz), float(smoothingLengthScale),
                                        out.ctypes.data_as(C.POINTER(C.c_float))), ctx)
     return out.reshape(2, M.size, order="F")
+
+
+def downsample_params(paramVals, nBins, device=0):
+    """Sub-media binning on the device (mcb_downsample_params; MATLAB's getDownsampledParamVals):
+    paramVals [3, n] float32 (mua, mus, g per voxel) -> (downsampled [3, nBins] float32,
+    binidx [n] uint8, 1-based)."""
+    ctx = context(device)
+    par = np.asfortranarray(np.asarray(paramVals, dtype=np.float32))
+    if par.ndim != 2 or par.shape[0] != 3:
+        raise ValueError("paramVals must be [3, n]")
+    n = par.shape[1]
+    out = np.zeros((3, int(nBins)), dtype=np.float32, order="F")
+    idx = np.zeros(n, dtype=np.uint8)
+    _check(lib().mcb_downsample_params(ctx, par.ctypes.data_as(C.POINTER(C.c_float)), n, int(nBins),
+                                       out.ctypes.data_as(C.POINTER(C.c_float)), idx.ctypes.data_as(C.POINTER(C.c_uint8))),
+           ctx)
+    return out, idx
 
 
 def probe_atomics(slots=1 << 20, device=0):

@@ -59,6 +59,21 @@ def philox(ctr, key):
     return list(o)
 
 
+def oracle_downsample(paramVals, nBins):
+    """CPU restatement of the sub-media binning: ([3 x n] float32, nBins) -> (downsampled [3 x nBins]
+    float32, binidx [n] uint8, 1-based)."""
+    par = np.asfortranarray(np.asarray(paramVals, dtype=np.float32))
+    n = par.shape[1]
+    out = np.zeros((3, int(nBins)), dtype=np.float32, order="F")
+    idx = np.zeros(n, dtype=np.uint8)
+    L = lib()
+    rc = L.orc_downsample(par.ctypes.data_as(C.POINTER(C.c_float)), C.c_long(n), C.c_int(int(nBins)),
+                          out.ctypes.data_as(C.POINTER(C.c_float)), idx.ctypes.data_as(C.POINTER(C.c_uint8)))
+    if rc != 0:
+        raise RuntimeError("oracle binning failed (%d)" % rc)
+    return out, idx
+
+
 def oracle_mc(mc_in, nthreads=0):
     mb = abi.McModelBuffers(mc_in)
     rb = abi.McResultBuffers(mc_in)

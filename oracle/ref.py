@@ -187,6 +187,30 @@ class RefMC:
         return res
 
 
+class RefDownsample:
+    """The reference's sub-media binning MEX (getDownsampledParamVals.c) on the host:
+    (paramVals [3 x n] single, nBins) -> (downsampled [3 x nBins] single, binidx [1 x n] uint8)."""
+
+    def __init__(self):
+        self.sh = shim()
+        self.lib = C.CDLL(os.path.join(REF_DIR, "libref_downsample.so"))
+        self.fn = self.lib.mexFunction
+
+    def run(self, paramVals, nBins):
+        sh = self.sh
+        a = sh.array(np.asfortranarray(np.asarray(paramVals, dtype=np.float32)))
+        b = sh.array(float(nBins))
+        try:
+            d, idx = sh.call(self.fn, 2, [a, b])
+            out = sh.to_numpy(d), sh.to_numpy(idx).reshape(-1)
+        finally:
+            sh.lib.mxDestroyArray(a)
+            sh.lib.mxDestroyArray(b)
+        sh.lib.mxDestroyArray(d)
+        sh.lib.mxDestroyArray(idx)
+        return out
+
+
 class RefHeat:
     """The reference heat MEX (finiteElementHeatPropagator.c) on the host cores. With
     libname="libmex_heat_cuda.so" it drives this library's heat MEX gateway instead."""
