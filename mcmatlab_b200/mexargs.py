@@ -30,14 +30,27 @@ _RESTRICTIVE = ("minScatterings", "maxScatterings", "minRefractions", "maxRefrac
                 "maxReflections", "minInterfaceTransitions", "maxInterfaceTransitions")
 
 
-def prepare_mc(mdl, simType=1, normals=None):
+def _fr_t_fd(mdl):
+    """Fluence rate, temperature and fractional damage grids of the model (getOpticalMediaProperties.m:23-30)."""
+    G = mdl.G
+    shape = G.M_raw.shape
+    T = np.broadcast_to(np.asarray(mdl.HS.T, dtype=np.float32), shape)
+    FD = np.broadcast_to((1 - np.exp(-np.asarray(mdl.HS.Omega, dtype=np.float64))).astype(np.float32), shape)
+    NFR = np.asarray(mdl.MC.NFR, dtype=np.float32)
+    FR = np.broadcast_to((mdl.MC.P * (NFR.sum(axis=3) if NFR.ndim == 4 else NFR)).astype(np.float32), shape)
+    return FR, T, FD
+
+
+def prepare_mc(mdl, simType=1, normals=None, downsample=None):
     """Flat MEX-level inputs for one MC run (runMonteCarlo.m + getOpticalMediaProperties.m).
 
     simType 1 reads model.MC; simType 2 (fluorescence) reads model.FMC, as MCmatlab.c:322-323
     does, and builds the fluorescence source from the excitation run's model.MC results
     (runMonteCarlo.m:119-166, prep.fluorescence_source), which it also stores in
     model.FMC.sourceDistribution. `normals` replaces prep.interface_normals (runMonteCarlo
-    passes the device version)."""
+    passes the device version); `downsample` performs the sub-media binning of media whose optical
+    properties depend on fluence rate, temperature or damage (runMonteCarlo passes
+    native.downsample_params)."""
     if simType not in (1, 2):
         raise ValueError("simType must be 1 (MC) or 2 (fluorescence MC)")
     G = mdl.G
@@ -70,13 +83,10 @@ def prepare_mc(mdl, simType=1, normals=None):
     if MC.useLightCollector and MC.boundaryType == 0:
         raise ValueError("Error: If boundaryType == 0, no photons can escape to be registered on the light collector. Disable light collector or change boundaryType.")
     media = G.mediaPropertiesFunc(G.mediaPropParams)
+    FR, T, FD = _fr_t_fd(mdl)
     mp = prep.optical_media_properties(media, G.M_raw, wl, MC.matchedInterfaces, G.dx, G.dy, G.dz, DC,
-                                       MC.smoothingLengthScale, normals)
+                                       MC.smoothingLengthScale, normals, FR=FR, T=T, FD=FD, downsample=downsample)
     if simType == 2:
-        T = np.broadcast_to(np.asarray(mdl.HS.T, dtype=np.float32), G.M_raw.shape)
-        FD = (1 - np.exp(-np.asarray(mdl.HS.Omega, dtype=np.float64))).astype(np.float32)
-        NFR = np.asarray(mdl.MC.NFR, dtype=np.float32)
-        FR = (mdl.MC.P * (NFR.sum(axis=3) if NFR.ndim == 4 else NFR)).astype(np.float32)
         MC.sourceDistribution = prep.fluorescence_source(media, G.M_raw, mdl.MC.NA, mdl.MC.wavelength, wl, FR, T, FD)
     SD = MC.sourceDistribution
     if np.ndim(SD) == 0:

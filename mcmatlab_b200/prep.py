@@ -178,65 +178,190 @@ def custom_phase_cdf(phase_func, wavelength):
     return np.concatenate([[0.0], np.cumsum(pdf) / np.sum(pdf)])
 
 
-def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0,
-                             normals=None):
-    """Per-sub-medium optical tables and the sub-medium grid (getOpticalMediaProperties.m).
+_TEST_WAVELENGTHS = np.linspace(100e-9, 10000e-9, 10)  # geometry.m:71 (as written there)
 
-    Media with FR/T/FD-dependent properties (nBins > 1, sub-media splitting) are not
-    supported by this preparation step; each medium maps to one sub-medium.
+
+def _test_grid():
+    FRs = np.concatenate([[0.0], np.logspace(-20, 20, 9)])
+    Ts = np.linspace(-100, 300, 10)
+    FDs = np.linspace(0, 1, 10)
+    return np.meshgrid(FRs, Ts, FDs, indexing="ij")
+
+
+def _varies(vals, axis):
+    """any(~isequaln(max(v,[],axis), min(v,[],axis))) with MATLAB's NaN-ignoring max/min."""
+    with np.errstate(all="ignore"):
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            hi = np.nanmax(vals, axis=axis)
+            lo = np.nanmin(vals, axis=axis)
+    return not np.array_equal(hi, lo, equal_nan=True)
+
+
+def dependence_flags(media):
+    """FRdependent, optTdependent, optFDdependent [nM, 5] (mua, mus, g, QY, ES) of the given media
+    (geometry.m:64-101): each property is sampled over wavelengths x (FR, T, FD) test grids and
+    flagged when it changes along the FR, T or FD axis."""
+    FR, T, FD = _test_grid()
+    nM = len(media)
+    flags = np.zeros((3, nM, 5), dtype=bool)
+    for iM, med in enumerate(media):
+        for iL, L in enumerate(_TEST_WAVELENGTHS):
+            for col, f in enumerate((med.mua, med.mus, med.g, med.QY, med.ES)):
+                if not callable(f) or _nargs(f) == 1:
+                    continue  # constant in FR, T and FD
+                vals = np.broadcast_to(np.asarray(f(L, FR, T, FD), dtype=np.float64), FR.shape)
+                for ax in range(3):
+                    flags[ax, iM, col] |= _varies(vals, ax)
+    return flags[0], flags[1], flags[2]
+
+
+def _eval_dep(f, wavelength, dependent, FRs, Ts, FDs):
+    """A medium property at one wavelength: over the medium's voxels when it depends on FR, T or
+    FD, else at (wavelength, 0, 0, 0) (getOpticalMediaProperties.m:64-84). The wavelength is a
+    Python float, so single-precision voxel arrays stay single as in MATLAB's mixed arithmetic."""
+    if not callable(f):
+        return f
+    if _nargs(f) == 1:
+        return f(wavelength)
+    return f(wavelength, FRs, Ts, FDs) if dependent else f(wavelength, 0.0, 0.0, 0.0)
+
+
+def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0,
+                             normals=None, FR=0.0, T=0.0, FD=0.0, downsample=None):
+    """Per-sub-medium optical tables and the sub-medium grid (getOpticalMediaProperties.m:1-244).
+
+    Media whose mua, mus or g depend on fluence rate, temperature or damage are evaluated per
+    voxel and split into nBins sub-media by the sub-media binning (getDownsampledParamVals; the
+    `downsample` callable, native.downsample_params on the device) on the first wavelength; later
+    wavelengths take the mean per bin (:147-197). FR, T and FD are grids (or scalars) of the
+    model's fluence rate, temperature and fractional damage.
     Returns a dict with mua, mus, g, n, CDFidx ([nSM, nL] float64), M (uint8, 1-based),
     CDFs ([201, nCDF] float64), interfaceNormals (float32 [2, L] or None) and the
     sub-media index range of the deposition criteria (1-based, may be inf).
     """
     wavelengths = np.atleast_1d(np.asarray(wavelengths, dtype=np.float64))
+    M_raw = np.asarray(M_raw)
     unique_media, M_trim = np.unique(M_raw, return_inverse=True)
     M_trim = M_trim.reshape(M_raw.shape) + 1
     trimmed = [mediaList[int(m) - 1] for m in unique_media]
-    names = [m.name for m in trimmed]
-    if len(set(names)) != len(names):
+    names_trim = [m.name for m in trimmed]
+    if len(set(names_trim)) != len(names_trim):
         raise ValueError("Error: Two media have the same name.")
     nM = len(trimmed)
     nL = wavelengths.size
-    for m in trimmed:
-        if getattr(m, "nBins", 1) != 1:
-            raise NotImplementedError("sub-media splitting (nBins > 1) is not supported")
-    mua = np.full((nM, nL), np.nan)
-    mus = np.full((nM, nL), np.nan)
-    g = np.full((nM, nL), np.nan)
-    n = np.full((nM, nL), np.nan)
-    CDFidx = np.full((nM, nL), np.nan)
+    nSMtotal = sum(int(getattr(m, "nBins", 1)) for m in trimmed)
+    if nSMtotal > 256:
+        raise ValueError("Error: The total number of (sub-)media may not exceed 256")
+    FRd, Td, FDd = dependence_flags(trimmed)
+    Mflat = M_trim.reshape(-1, order="F")
+    shape = M_raw.shape
+    FRf = np.broadcast_to(np.asarray(FR, dtype=np.float32), shape).reshape(-1, order="F")
+    Tf = np.broadcast_to(np.asarray(T, dtype=np.float32), shape).reshape(-1, order="F")
+    FDf = np.broadcast_to(np.asarray(FD, dtype=np.float32), shape).reshape(-1, order="F")
+    mua = np.full((nSMtotal, nL), np.nan)
+    mus = np.full((nSMtotal, nL), np.nan)
+    g = np.full((nSMtotal, nL), np.nan)
+    n = np.full((nSMtotal, nL), np.nan)
+    CDFidx = np.full((nSMtotal, nL), np.nan)
+    names = [None] * nSMtotal
+    Msub = np.zeros(Mflat.size, dtype=np.int64)
     cdfs = []
     minSub, maxSub = np.inf, np.inf
+    iSM = 0  # 0-based first sub-medium of the current medium
     for iM, med in enumerate(trimmed):
+        idx = np.nonzero(Mflat == iM + 1)[0]
+        dep = [FRd[iM, c] or Td[iM, c] or FDd[iM, c] for c in range(3)]
+        FRs, Ts, FDs = FRf[idx], Tf[idx], FDf[idx]
+        nSM = int(getattr(med, "nBins", 1))
+        binidx = None
         for iL, L in enumerate(wavelengths):
-            a = float(np.float32(eval_optical(med.mua, L)))
-            s = float(np.float32(eval_optical(med.mus, L)))
-            gv = eval_optical(med.g, L)
-            gv = float(np.float32(gv)) if gv is not None else math.nan
-            if not math.isfinite(a):
+            vals = []
+            for c, (f, what) in enumerate(((med.mua, "mua"), (med.mus, "mus"), (med.g, "g"))):
+                try:
+                    v = _eval_dep(f, float(L), dep[c], FRs, Ts, FDs)
+                except Exception as e:
+                    raise ValueError("Error: The %s function of medium %s is throwing an error: %s" % (what, med.name, e))
+                v = np.float32(math.nan) if v is None else v
+                vals.append(np.asarray(v, dtype=np.float32))
+            muav, musv, gv = vals
+            if np.any(~np.isfinite(muav)):
                 raise ValueError("The mua function of medium %s returns NaN or Inf values." % med.name)
-            if not math.isfinite(s):
+            if np.any(~np.isfinite(musv)):
                 raise ValueError("The mus function of medium %s returns NaN or Inf values." % med.name)
-            if math.isfinite(gv):
-                g[iM, iL] = gv
+            if np.any(~np.isfinite(gv)) and not np.all(~np.isfinite(gv)):
+                raise ValueError("The g function of medium %s returns NaN or Inf values in some, but not all voxels." % med.name)
+            useg = not np.all(~np.isfinite(gv))
+            if useg:
+                cidx = math.nan
             else:
                 cdf = custom_phase_cdf(med.customPhaseFunc, L)
-                idx = None
+                cidx = None
                 for k, c in enumerate(cdfs):
                     if np.array_equal(c, cdf):
-                        idx = k
+                        cidx = k
                         break
-                if idx is None:
+                if cidx is None:
                     cdfs.append(cdf)
-                    idx = len(cdfs) - 1
-                CDFidx[iM, iL] = idx
-            mua[iM, iL] = a
-            mus[iM, iL] = s
-            n[iM, iL] = float(eval_optical(med.n, L))
-        if DC.minMediumIdxToConsider == unique_media[iM]:
-            minSub = iM + 1
-        if DC.maxMediumIdxToConsider == unique_media[iM]:
-            maxSub = iM + 1
+                    cidx = len(cdfs) - 1
+            nval = float(eval_optical(med.n, L))
+            if DC.minMediumIdxToConsider == unique_media[iM]:
+                minSub = iSM + 1
+            if DC.maxMediumIdxToConsider == unique_media[iM]:
+                maxSub = iSM + nSM
+            rows = slice(iSM, iSM + nSM)
+            if muav.ndim == 0 and musv.ndim == 0 and gv.ndim == 0:
+                if iL == 0:
+                    names[rows] = [med.name] * nSM
+                    Msub[idx] = iSM + 1
+                mua[rows, iL] = float(muav)
+                mus[rows, iL] = float(musv)
+                if useg:
+                    g[rows, iL] = float(gv)
+                n[rows, iL] = nval
+                CDFidx[rows, iL] = cidx
+            elif iL == 0:
+                # one binning, from the first wavelength (getOpticalMediaProperties.m:148-165)
+                if downsample is None:
+                    raise ValueError("medium %s depends on FR, T or FD: splitting it needs the sub-media binning "
+                                     "(pass downsample=native.downsample_params)" % med.name)
+                par = np.zeros((3, idx.size), dtype=np.float32)
+                par[0] = muav
+                par[1] = musv
+                par[2] = gv if useg else 0.0
+                reps, lab = downsample(np.asfortranarray(par), nSM)
+                reps = np.asarray(reps, dtype=np.float32)
+                order = np.lexsort((reps[2], reps[1], reps[0]))  # sortrows of the representatives
+                rank = np.empty(nSM, dtype=np.int64)
+                rank[order] = np.arange(nSM)
+                binidx = rank[np.asarray(lab, dtype=np.int64) - 1] + 1
+                Msub[idx] = iSM + binidx
+                reps = reps[:, order]
+                names[rows] = [med.name] * nSM
+                mua[rows, 0] = reps[0].astype(np.float64)
+                mus[rows, 0] = reps[1].astype(np.float64)
+                if useg:
+                    g[rows, 0] = reps[2].astype(np.float64)
+                n[rows, 0] = nval
+                CDFidx[rows, 0] = cidx
+            else:
+                # later wavelengths: the mean of the new values in each bin (:167-196)
+                present = np.zeros(nSM, dtype=bool)
+                present[np.unique(Msub[idx]) - 1 - iSM] = True
+                for k in range(nSM):
+                    if present[k]:
+                        sel = binidx == k + 1
+                        mua[iSM + k, iL] = float(muav) if muav.ndim == 0 else float(np.mean(muav[sel].astype(np.float64)))
+                        mus[iSM + k, iL] = float(musv) if musv.ndim == 0 else float(np.mean(musv[sel].astype(np.float64)))
+                        g[iSM + k, iL] = float(gv) if gv.ndim == 0 else float(np.mean(gv[sel].astype(np.float64)))
+                    else:
+                        mua[iSM + k, iL] = mua[iSM, iL]
+                        mus[iSM + k, iL] = mus[iSM, iL]
+                        g[iSM + k, iL] = g[iSM, iL]
+                    n[iSM + k, iL] = nval
+                    CDFidx[iSM + k, iL] = cidx
+        iSM += nSM
     if matchedInterfaces:
         n[:] = 1.0
     if np.any(~np.isfinite(mua)) or np.any(mua <= 0):
@@ -247,7 +372,7 @@ def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, d
         raise ValueError("Error: A medium has invalid g. Must be finite, real and between -1 and 1, or NaN.")
     if np.any(np.isnan(n)) or np.any(n < 1):
         raise ValueError("Error: A medium has invalid n. Must not be NaN, must be real and at least 1.")
-    M = np.asfortranarray(M_trim.astype(np.uint8))
+    M = np.asfortranarray(Msub.reshape(shape, order="F").astype(np.uint8))
     # `normals` may supply another implementation of interface_normals (the device one)
     normals = None if matchedInterfaces else (normals or interface_normals)(M, n, dx, dy, dz, smoothingLengthScale)
     CDFs = np.stack(cdfs, axis=1) if cdfs else np.zeros((0, 0))
@@ -299,14 +424,14 @@ def fluorescence_source(mediaList, M_raw, NA, Ls_E, Ls_F, FR, T, FD):
         acc = np.zeros(idx.size)
         for iLE in range(nLE):
             try:
-                qy = _eval_yield(med.QY, Ls_E[iLE], FRf[idx], Tf[idx], FDf[idx])
+                qy = _eval_yield(med.QY, float(Ls_E[iLE]), FRf[idx], Tf[idx], FDf[idx])
             except Exception as e:
                 raise ValueError("Error: The QY function of medium %s is throwing an error: %s" % (med.name, e))
             acc = acc + NAf[idx, iLE] * np.asarray(qy, dtype=np.float64) * Ls_E[iLE]
         Fphotons[idx] = acc
         for iLF in range(nLF):
             try:
-                es = _eval_yield(med.ES, Ls_F[iLF], FRf[idx], Tf[idx], FDf[idx])
+                es = _eval_yield(med.ES, float(Ls_F[iLF]), FRf[idx], Tf[idx], FDf[idx])
             except Exception as e:
                 raise ValueError("Error: The ES function of medium %s is throwing an error: %s" % (med.name, e))
             emSp[idx, iLF] = np.asarray(es, dtype=np.float64)

@@ -25,11 +25,36 @@ def _squeeze_last(a, nL):
 def runMonteCarlo(model, *args):
     simType = 2 if "fluorescence" in args else 1
     MC = model.FMC if simType == 2 else model.MC
-    if simType == 1 and model.MC.FRdepIterations:
-        raise NotImplementedError("fluence-rate-dependent iterations are not part of this library")
     model.G.updateGeometry()
+    if simType == 1 and MC.FRdepIterations > 0:
+        # fluence-rate dependent media: nIterations runs with 1/2^(n-1), ..., 1/2, 1 of the
+        # requested packets (or time), each re-binning the media on the previous fluence rate
+        # (runMonteCarlo.m:81-113)
+        nIt = int(MC.FRdepIterations)
+        timed = math.isnan(MC.nPhotonsRequested)
+        req = MC.simulationTimeRequested if timed else MC.nPhotonsRequested
+        for i in range(nIt):
+            part = req * 0.5 ** (nIt - 1 - i)
+            if timed:
+                MC.simulationTimeRequested = part
+            else:
+                MC.nPhotonsRequested = part
+            _run_once(model, simType)
+            if i < nIt - 1:
+                MC.FR = MC.P * np.asarray(MC.NFR)
+        if timed:
+            MC.simulationTimeRequested = req
+        else:
+            MC.nPhotonsRequested = req
+        return model
+    return _run_once(model, simType)
+
+
+def _run_once(model, simType):
+    MC = model.FMC if simType == 2 else model.MC
     dev = MC.GPUdevice
-    mc_in = mexargs.prepare_mc(model, simType, normals=lambda *a: native.interface_normals(*a, device=dev))
+    mc_in = mexargs.prepare_mc(model, simType, normals=lambda *a: native.interface_normals(*a, device=dev),
+                               downsample=lambda par, nb: native.downsample_params(par, nb, device=dev))
     out = native.mc_run(mc_in, device=dev)
     nL = np.asarray(mc_in["mua"]).shape[1]
     if simType == 1:
