@@ -6,8 +6,12 @@ Follows the reference: thermal media (:31), per-medium initial maxima (:39-49), 
 HS.dtFactor when set), time vectors (:112-128), dT/dt arrays (:132), sensors (:135-150), then
 for each pulse the illumination and diffusion phases and the end phase, each as nUpdates
 stepper calls (:240-420). The grids stay resident on the GPU across the update calls
-(mcb_heat_state_*); the reference re-uploads them on every MEX call. Plotting, movies and
-property recalculation are not part of this library.
+(mcb_heat_state_*); the reference re-uploads them on every MEX call. Every
+HS.mediaPropRecalcPeriod updates the media are recalculated as heatSimParamsRecalc does
+(:516-541): with temperature or damage dependent optical properties the MC (and the fluorescence
+MC, if it ran) is re-run on the GPU at the current T and Omega, then the thermal media are
+re-binned and the heat source rebuilt, and the stepper continues from the current grids.
+Plotting and movies are not part of this library.
 """
 from __future__ import annotations
 
@@ -29,7 +33,14 @@ def simulateHeatDistribution(model):
     T[...] = np.asarray(HS.T, dtype=np.float32)
     first = np.ndim(HS.maxMediaTemps) == 0 and math.isnan(HS.maxMediaTemps)
     media = G.mediaPropertiesFunc(G.mediaPropParams)
-    th = prep.thermal_media_properties(media, G.M_raw, T, 0.0)
+    dev = MC.GPUdevice
+
+    def binning(par, nb):
+        return native.downsample_params(par, nb, device=dev)
+
+    def fd_grid():
+        return (1 - np.exp(-np.asarray(HS.Omega, dtype=np.float64))).astype(np.float32) if np.ndim(HS.Omega) else np.float32(0.0)
+    th = prep.thermal_media_properties(media, G.M_raw, T, fd_grid(), downsample=binning)
     HS.mediaProperties = {"name": th["names"], "VHC": th["VHC"], "TC": th["TC"], "A": th["A"], "E": th["E"]}
     HS.M = th["M"]
     nM = len(th["VHC"])
@@ -84,25 +95,62 @@ def simulateHeatDistribution(model):
                                        lightsOn, steps, dt)
 
     state = native.HeatState(T, HS.Omega if damage else None, params(True, 1, dtOn), G.nx, G.ny, G.nz,
-                             device=MC.GPUdevice)
+                             device=dev)
     maxT = np.asarray(HS.maxMediaTemps, dtype=np.float64).copy()
+    period = int(HS.mediaPropRecalcPeriod)
+    FRd, Td, FDd = prep.dependence_flags([media[int(m) - 1] for m in np.unique(G.M_raw)])
+    thmT, thmFD = prep.thermal_dependence_flags([media[int(m) - 1] for m in np.unique(G.M_raw)])
+    opt_dep = bool(np.any(Td | FDd))
+    thm_dep = bool(np.any(thmT | thmFD))
 
-    def run(n_updates, steps, dt, lights):
+    def recalc():
+        """heatSimParamsRecalc (simulateHeatDistribution.m:516-541) at the current grids."""
+        nonlocal state, th, c, Q, generation
+        generation += 1
+        Tc, Oc = state.read()
+        HS.T = Tc
+        if damage:
+            HS.Omega = Oc
+        if opt_dep:
+            silent = MC.silentMode
+            MC.silentMode = True
+            model.runMonteCarlo()
+            MC.silentMode = silent
+            if not math.isnan(model.FMC.simulationTime):
+                model.runMonteCarlo("fluorescence")
+        if opt_dep or thm_dep:
+            th = prep.thermal_media_properties(media, G.M_raw, Tc, fd_grid(), downsample=binning)
+            HS.mediaProperties = {"name": th["names"], "VHC": th["VHC"], "TC": th["TC"], "A": th["A"], "E": th["E"]}
+            HS.M = th["M"]
+        NA = np.asarray(MC.normalizedAbsorption, dtype=np.float64)
+        c, Q = prep.calc_dTdt_arrays(th["VHC"], th["TC"], G.dx, G.dy, G.dz, NA.sum(axis=3) if NA.ndim == 4 else NA,
+                                     MC.P, th["M"])
+        state.close()
+        state = native.HeatState(Tc, Oc if damage else None, params(True, 1, dtOn), G.nx, G.ny, G.nz, device=dev)
+
+    generation = 0
+
+    def run(n_updates, steps, dt, lights, first_idx):
         nonlocal sensorTemps
-        hp = params(lights, steps, dt)
-        for _ in range(n_updates):
+        hp, built = params(lights, steps, dt), generation
+        for i in range(n_updates):
+            if built != generation:  # media recalculated: new media grid, coefficients and source
+                hp, built = params(lights, steps, dt), generation
             sens, mx = state.step(hp)
             maxT[:] = np.maximum(maxT, mx.ravel().astype(np.float64))
             if li is not None:
                 sensorTemps = sens if sensorTemps is None else np.concatenate([sensorTemps[:, :-1], sens], axis=1)
+            if period > 0 and (first_idx + i + 1) % period == 0:
+                recalc()
 
     try:
-        for _ in range(HS.nPulses):
+        per_pulse = nUon + nUoff
+        for j in range(HS.nPulses):
             if HS.durationOn != 0:
-                run(nUon, nTon, dtOn, True)
+                run(nUon, nTon, dtOn, True, j * per_pulse)
             if HS.durationOff != 0:
-                run(nUoff, nToff, dtOff, False)
-        run(nUend, nTend, dtEnd, False)
+                run(nUoff, nToff, dtOff, False, j * per_pulse + nUon)
+        run(nUend, nTend, dtEnd, False, HS.nPulses * per_pulse)
         Tn, On = state.read()
     finally:
         state.close()

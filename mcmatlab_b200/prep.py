@@ -448,24 +448,90 @@ def fluorescence_source(mediaList, M_raw, NA, Ls_E, Ls_F, FR, T, FD):
     return np.asfortranarray(S.reshape(tuple(shape) + (nLF,), order="F"))
 
 
-def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0):
-    """VHC, TC, A, E per sub-medium and the sub-medium grid (getThermalMediaProperties.m).
+def thermal_dependence_flags(media):
+    """thmTdependent, thmFDdependent [nM, 2] (VHC, TC) as geometry.m:95-100 computes them: each
+    property is evaluated on the (FR, T, FD) test grids and flagged when it changes along the
+    grids' first axis (thmTdependent) or second axis (thmFDdependent). As written there, the first
+    axis is the fluence-rate axis, so a temperature-dependent property shows up in thmFDdependent
+    and thmTdependent stays false; the recalculation test uses their union (:520, :534)."""
+    FR, T, FD = _test_grid()
+    nM = len(media)
+    thmT = np.zeros((nM, 2), dtype=bool)
+    thmFD = np.zeros((nM, 2), dtype=bool)
+    for iM, med in enumerate(media):
+        for col, f in enumerate((med.VHC, med.TC)):
+            if not callable(f):
+                continue
+            vals = np.broadcast_to(np.asarray(f(T, FD), dtype=np.float64), FR.shape)
+            thmT[iM, col] = _varies(vals, 0)
+            thmFD[iM, col] = _varies(vals, 1)
+    return thmT, thmFD
 
-    Only temperature/damage-independent thermal properties are supported (nBins = 1).
+
+def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0, downsample=None):
+    """VHC, TC, A, E per sub-medium and the sub-medium grid (getThermalMediaProperties.m:27-96).
+
+    VHC and TC are evaluated per voxel at the voxel's temperature and fractional damage; every
+    medium is then split into nBins sub-media by the sub-media binning of the (VHC, TC, 1) triples
+    (the `downsample` callable, native.downsample_params on the device; only needed when a
+    medium's values differ between voxels, otherwise every voxel keeps the common value), with
+    the representatives sorted as MATLAB's sortrows orders them.
     """
+    M_raw = np.asarray(M_raw)
     unique_media, M_trim = np.unique(M_raw, return_inverse=True)
     M_trim = M_trim.reshape(M_raw.shape) + 1
     trimmed = [mediaList[int(m) - 1] for m in unique_media]
-    VHC = np.array([float(np.float32(eval_thermal(m.VHC, T, FD))) for m in trimmed])
-    TC = np.array([float(np.float32(eval_thermal(m.TC, T, FD))) for m in trimmed])
-    if np.any(~np.isfinite(VHC)) or np.any(VHC <= 0):
-        raise ValueError("The VHC function of a medium returns values that are not finite and positive.")
-    if np.any(~np.isfinite(TC)) or np.any(TC <= 0):
-        raise ValueError("The TC function of a medium returns values that are not finite and positive.")
-    A = np.array([float(m.A) for m in trimmed])
-    E = np.array([float(m.E) for m in trimmed])
-    return dict(VHC=VHC, TC=TC, A=A, E=E, M=np.asfortranarray(M_trim.astype(np.uint8)),
-                names=[m.name for m in trimmed])
+    names_trim = [m.name for m in trimmed]
+    if len(set(names_trim)) != len(names_trim):
+        raise ValueError("Error: Two media have the same name.")
+    nSMtotal = sum(int(getattr(m, "nBins", 1)) for m in trimmed)
+    if nSMtotal > 256:
+        raise ValueError("Error: The total number of (sub-)media may not exceed 256")
+    shape = M_raw.shape
+    Mflat = M_trim.reshape(-1, order="F")
+    Tf = np.broadcast_to(np.asarray(T, dtype=np.float32), shape).reshape(-1, order="F")
+    FDf = np.broadcast_to(np.asarray(FD, dtype=np.float32), shape).reshape(-1, order="F")
+    VHC = np.full(nSMtotal, np.nan)
+    TC = np.full(nSMtotal, np.nan)
+    A = np.full(nSMtotal, np.nan)
+    E = np.full(nSMtotal, np.nan)
+    names = [None] * nSMtotal
+    Msub = np.zeros(Mflat.size, dtype=np.int64)
+    iSM = 0
+    for iM, med in enumerate(trimmed):
+        idx = np.nonzero(Mflat == iM + 1)[0]
+        par = np.ones((3, idx.size), dtype=np.float32)
+        for row, (f, what) in enumerate(((med.VHC, "VHC"), (med.TC, "TC"))):
+            try:
+                v = f(Tf[idx], FDf[idx]) if callable(f) else f
+            except Exception as e:
+                raise ValueError("Error: The %s function of medium %s is throwing an error: %s" % (what, med.name, e))
+            par[row] = np.asarray(v, dtype=np.float32)
+            if np.any(~np.isfinite(par[row])) or np.any(par[row] <= 0):
+                raise ValueError("The %s function of medium %s returns values that are not finite and positive." % (what, med.name))
+        nSM = int(getattr(med, "nBins", 1))
+        if np.all(par == par[:, :1]):
+            reps = np.repeat(par[:, :1], nSM, axis=1)  # the binning of a single value
+            lab = np.ones(idx.size, dtype=np.int64)
+        else:
+            if downsample is None:
+                raise ValueError("medium %s has voxel-dependent thermal properties: splitting it needs the sub-media "
+                                 "binning (pass downsample=native.downsample_params)" % med.name)
+            reps, lab = downsample(np.asfortranarray(par), nSM)
+            reps = np.asarray(reps, dtype=np.float32)
+        order = np.lexsort((reps[2], reps[1], reps[0]))
+        rank = np.empty(nSM, dtype=np.int64)
+        rank[order] = np.arange(nSM)
+        Msub[idx] = iSM + rank[np.asarray(lab, dtype=np.int64) - 1] + 1
+        reps = reps[:, order]
+        names[iSM:iSM + nSM] = [med.name] * nSM
+        VHC[iSM:iSM + nSM] = reps[0].astype(np.float64)
+        TC[iSM:iSM + nSM] = reps[1].astype(np.float64)
+        A[iSM:iSM + nSM] = float(med.A)
+        E[iSM:iSM + nSM] = float(med.E)
+        iSM += nSM
+    return dict(VHC=VHC, TC=TC, A=A, E=E, M=np.asfortranarray(Msub.reshape(shape, order="F").astype(np.uint8)),
+                names=names)
 
 
 def calc_dTdt_arrays(VHC, TC, dx, dy, dz, NA_sum, P, M1):

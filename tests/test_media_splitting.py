@@ -78,3 +78,33 @@ def test_split_needs_the_binning():
     with pytest.raises(ValueError, match="256"):
         prep.optical_media_properties(too_many, np.array([[[1, 2]]], dtype=float), [500.0], True, 0.1, 0.1, 0.1,
                                       depositionCriteria())
+
+
+def test_thermal_splitting_and_flags(oracle_lib):
+    ds = _oracle_ds(oracle_lib)
+    media = [mm.mediumProperties(name="fixed", VHC=3.9, TC=0.0037, nBins=2),
+             mm.mediumProperties(name="soft", VHC=lambda T, FD: 3.9 * (1 + 0.002 * (T - 37.0)), TC=0.0037, nBins=5,
+                                 A=1e10, E=1e5)]
+    thmT, thmFD = prep.thermal_dependence_flags(media)
+    # geometry.m tests the first grid axis (fluence rate) for T and the second (temperature) for FD
+    assert not thmT.any() and thmFD[1, 0] and not thmFD[1, 1] and not thmFD[0].any()
+    rng = np.random.default_rng(4)
+    shape = (6, 6, 6)
+    M_raw = np.ones(shape)
+    M_raw[:, :, 3:] = 2
+    T = rng.uniform(37, 80, shape).astype(np.float32)
+    th = prep.thermal_media_properties(media, M_raw, T, 0.0, downsample=ds)
+    assert th["VHC"].shape == (7,) and np.all(th["VHC"][:2] == np.float32(3.9))
+    assert np.all(th["M"][M_raw == 1] == 1)
+    sub = th["M"][M_raw == 2].astype(int)
+    assert sub.min() >= 3 and sub.max() <= 7 and np.all(np.diff(th["VHC"][2:]) >= 0)
+    np.testing.assert_array_equal(th["A"], [0, 0, 1e10, 1e10, 1e10, 1e10, 1e10])
+    idx = np.nonzero((M_raw == 2).reshape(-1, order="F"))[0]
+    Tv = T.reshape(-1, order="F")[idx]
+    par = np.stack([3.9 * (1 + 0.002 * (Tv - 37.0)), np.full(idx.size, 0.0037, np.float32),
+                    np.ones(idx.size, np.float32)]).astype(np.float32)
+    reps, lab = ds(par, 5)
+    order = np.lexsort((reps[2], reps[1], reps[0]))
+    np.testing.assert_array_equal(th["VHC"][2:], reps[0, order].astype(np.float64))
+    with pytest.raises(ValueError, match="sub-media binning"):
+        prep.thermal_media_properties(media, M_raw, T, 0.0)
