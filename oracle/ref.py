@@ -189,11 +189,13 @@ class RefMC:
 
 class RefDownsample:
     """The reference's sub-media binning MEX (getDownsampledParamVals.c) on the host:
-    (paramVals [3 x n] single, nBins) -> (downsampled [3 x nBins] single, binidx [1 x n] uint8)."""
+    (paramVals [3 x n] single, nBins) -> (downsampled [3 x nBins] single, binidx [1 x n] uint8).
+    With libname="libmex_ds_cuda.so" the same harness drives this library's gateway
+    (mcmatlab_b200/mex/getDownsampledParamVals_CUDA.c)."""
 
-    def __init__(self):
+    def __init__(self, libname="libref_downsample.so"):
         self.sh = shim()
-        self.lib = C.CDLL(os.path.join(REF_DIR, "libref_downsample.so"))
+        self.lib = C.CDLL(os.path.join(REF_DIR, libname))
         self.fn = self.lib.mexFunction
 
     def run(self, paramVals, nBins):

@@ -41,6 +41,31 @@ def test_mc_gateway_matches_reference(name, gateways):
     assert ok, rep
 
 
+def test_binning_gateway_matches_reference_build(gateways):
+    """getDownsampledParamVals through the gateway (device binning) against the reference MEX's
+    own outputs: bit for bit."""
+    import dscases
+    from oracle import ref
+    gw = ref.RefDownsample("libmex_ds_cuda.so")
+    cases = dscases.cases(count=24, seed=3)
+    if ref_build_present():
+        R = ref.RefDownsample()
+        for par, nb in cases:
+            a, b = R.run(par, nb), gw.run(par, nb)
+            np.testing.assert_array_equal(b[0], a[0])
+            np.testing.assert_array_equal(b[1], a[1])
+    else:
+        from oracle import orc
+        for par, nb in cases:
+            a, b = orc.oracle_downsample(par, nb), gw.run(par, nb)
+            np.testing.assert_array_equal(b[0], a[0])
+            np.testing.assert_array_equal(b[1].reshape(-1), a[1])
+
+
+def ref_build_present():
+    return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_downsample.so"))
+
+
 def test_heat_gateway_matches_reference(gateways):
     _, gw = gateways
     gold = np.load(os.path.join(GOLD, "heat_ref.npz"))
