@@ -233,7 +233,9 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
 }
 
 // lambda^n, dJ/dQ and dJ/dc of one reversed step (7-point stencil over every voxel).
-__global__ void __launch_bounds__(512) adj_assemble_kernel(AdjDev a) {
+// bounded for 3 blocks of 512 threads per SM: 40 registers with a few spills, which lets more
+// row blocks share an SM and measured 3% faster reverse sweeps than 57 registers without spills
+__global__ void __launch_bounds__(512, 3) adj_assemble_kernel(AdjDev a) {
   const HeatDev &h = a.h;
   __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
   const int nM = h.nM, nM2 = nM * nM;
