@@ -346,7 +346,10 @@ def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, d
                 n[rows, 0] = nval
                 CDFidx[rows, 0] = cidx
             else:
-                # later wavelengths: the mean of the new values in each bin (:167-196)
+                # later wavelengths: the mean of the new values in each bin (:167-196); a medium
+                # that took one value on the first wavelength has all its voxels in its first bin
+                if binidx is None:
+                    binidx = np.ones(idx.size, dtype=np.int64)
                 present = np.zeros(nSM, dtype=bool)
                 present[np.unique(Msub[idx]) - 1 - iSM] = True
                 for k in range(nSM):
