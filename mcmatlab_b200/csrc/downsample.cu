@@ -221,7 +221,7 @@ extern "C" mcb_status mcb_downsample_params(mcb_ctx *ctx, const float *paramVals
     ds_init_kernel<<<grid, 256, 0, st>>>(a);
     ds_first_center_kernel<<<1, 1, 0, st>>>(a);
     ds_first_kernel<<<grid, 256, 0, st>>>(a);
-    ds_pick_kernel<<<1, 1, 0, st>>>(a, 0, 0);
+    if (nBins > 1) ds_pick_kernel<<<1, 1, 0, st>>>(a, 0, 0);  // writes the second representative
     for (int j = 1; j < nBins; j++) {
       ds_update_kernel<<<grid, 256, 0, st>>>(a, j);
       if (j + 1 == nBins) break;  // the last centre needs no successor
