@@ -25,4 +25,6 @@ def cases(count=120, seed=0):
             nb = int(rng.integers(1, 12))  # possibly more bins than points
         out.append((np.asfortranarray(par), nb))
     out.append((np.ones((3, 50), np.float32, order="F"), 5))  # nothing varies
+    out.append((np.asfortranarray(rng.uniform(0, 1, (3, 300)).astype(np.float32)), 1))  # one bin
+    out.append((np.asfortranarray(rng.uniform(0, 1, (3, 300)).astype(np.float32)), 255))  # the most bins
     return out
