@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
       }
     }
     if (__all_sync(0xffffffffu, retired && !P.alive)) break;
-    // 3. one propagation sub-step, then the scattering event if the free path is used up
+    // 3. one propagation sub-step for every packet with free path left
     if (P.alive) {
       if (P.stepLeft > 0) {
         const int mj = GRAD ? P.med : 0;
@@ -312,7 +312,19 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
         }
         if (++P.nsteps >= kMaxFreeSteps) P.alive = false;
       }
-      if (P.alive && !(P.stepLeft > 0)) {
+    }
+    // 4. scattering events in groups: a packet whose free path is used up waits (no sub-step)
+    //    until enough lanes of its warp are waiting too, or no lane can take a sub-step, so the
+    //    long scattering code runs with most lanes active. A packet's events and random draws do
+    //    not change, only when its warp performs them. Measured on the 100^3 cube / 256^3
+    //    8-medium cube: groups of 8 gave the plain kernel 9.5% / 6% more packets/s, groups of 16
+    //    the gradient kernel 4.5%.
+    {
+      constexpr int kScatterGroup = GRAD ? 16 : 8;
+      const bool want = P.alive && !(P.stepLeft > 0);
+      const unsigned waiting = __ballot_sync(0xffffffffu, want);
+      const unsigned stepping = __ballot_sync(0xffffffffu, P.alive && P.stepLeft > 0);
+      if (want && (__popc(waiting) >= kScatterGroup || stepping == 0)) {
         if (P.weight < kThreshold) {
           if (rnd(P, *I) <= kChance) P.weight /= kChance;
           else P.alive = false;
