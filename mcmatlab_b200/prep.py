@@ -49,6 +49,16 @@ def eval_optical(f, wavelength):
     return f
 
 
+def elementwise(f, *args):
+    """f applied to array arguments: called once on the arrays, as the reference requires of
+    FR/T/FD-dependent property functions (element-wise arithmetic, getOpticalMediaProperties.m:
+    67-83); a function written for scalars is applied element by element instead."""
+    try:
+        return f(*args)
+    except (TypeError, ValueError):
+        return np.vectorize(f, otypes=[np.float64])(*args)
+
+
 def eval_thermal(f, T=37.0, FD=0.0):
     """Thermal property given as a number or f(T, FD) (mediumProperties.m:180-207)."""
     if callable(f):
@@ -211,7 +221,7 @@ def dependence_flags(media):
             for col, f in enumerate((med.mua, med.mus, med.g, med.QY, med.ES)):
                 if not callable(f) or _nargs(f) == 1:
                     continue  # constant in FR, T and FD
-                vals = np.broadcast_to(np.asarray(f(L, FR, T, FD), dtype=np.float64), FR.shape)
+                vals = np.broadcast_to(np.asarray(elementwise(f, L, FR, T, FD), dtype=np.float64), FR.shape)
                 for ax in range(3):
                     flags[ax, iM, col] |= _varies(vals, ax)
     return flags[0], flags[1], flags[2]
@@ -225,7 +235,7 @@ def _eval_dep(f, wavelength, dependent, FRs, Ts, FDs):
         return f
     if _nargs(f) == 1:
         return f(wavelength)
-    return f(wavelength, FRs, Ts, FDs) if dependent else f(wavelength, 0.0, 0.0, 0.0)
+    return elementwise(f, wavelength, FRs, Ts, FDs) if dependent else f(wavelength, 0.0, 0.0, 0.0)
 
 
 def optical_media_properties(mediaList, M_raw, wavelengths, matchedInterfaces, dx, dy, dz, DC, smoothingLengthScale=0.0,
@@ -389,7 +399,7 @@ def _eval_yield(f, wavelength, FR, T, FD):
     or f(wavelength, FR, T, FD) with FR, T, FD the voxels' arrays (element-wise, as the
     reference requires of four-argument functions, runMonteCarlo.m:135-137)."""
     if callable(f):
-        return f(wavelength) if _nargs(f) == 1 else f(wavelength, FR, T, FD)
+        return f(wavelength) if _nargs(f) == 1 else elementwise(f, wavelength, FR, T, FD)
     return f
 
 
@@ -465,7 +475,7 @@ def thermal_dependence_flags(media):
         for col, f in enumerate((med.VHC, med.TC)):
             if not callable(f):
                 continue
-            vals = np.broadcast_to(np.asarray(f(T, FD), dtype=np.float64), FR.shape)
+            vals = np.broadcast_to(np.asarray(elementwise(f, T, FD), dtype=np.float64), FR.shape)
             thmT[iM, col] = _varies(vals, 0)
             thmFD[iM, col] = _varies(vals, 1)
     return thmT, thmFD
@@ -506,7 +516,7 @@ def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0, downsample=None):
         par = np.ones((3, idx.size), dtype=np.float32)
         for row, (f, what) in enumerate(((med.VHC, "VHC"), (med.TC, "TC"))):
             try:
-                v = f(Tf[idx], FDf[idx]) if callable(f) else f
+                v = elementwise(f, Tf[idx], FDf[idx]) if callable(f) else f
             except Exception as e:
                 raise ValueError("Error: The %s function of medium %s is throwing an error: %s" % (what, med.name, e))
             par[row] = np.asarray(v, dtype=np.float32)

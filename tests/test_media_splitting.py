@@ -108,3 +108,22 @@ def test_thermal_splitting_and_flags(oracle_lib):
     np.testing.assert_array_equal(th["VHC"][2:], reps[0, order].astype(np.float64))
     with pytest.raises(ValueError, match="sub-media binning"):
         prep.thermal_media_properties(media, M_raw, T, 0.0)
+
+
+def test_scalar_property_functions_apply_elementwise(oracle_lib):
+    """A property function written for scalars (math module, `if`) is applied voxel by voxel."""
+    import math
+    ds = _oracle_ds(oracle_lib)
+    med = [mm.mediumProperties(name="s", mua=lambda wl, FR, T, FD: 1.0 + 9.0 * math.exp(-FR / 50.0),
+                               mus=10.0, g=0.9, n=1.0, nBins=4,
+                               VHC=lambda T, FD: 3.9 + (0.5 if T > 50 else 0.0), TC=0.0037)]
+    FRd, _, _ = prep.dependence_flags(med)
+    assert FRd[0, 0]
+    shape = (5, 5, 5)
+    FR = np.linspace(0, 300, 125, dtype=np.float32).reshape(shape)
+    mp = prep.optical_media_properties(med, np.ones(shape), [500.0], True, 0.1, 0.1, 0.1, depositionCriteria(),
+                                       FR=FR, T=37.0, downsample=ds)
+    assert np.unique(mp["M"]).size == 4 and mp["mua"][:, 0].max() <= 10.0
+    T = np.where(np.arange(125).reshape(shape) % 2 == 0, 40.0, 60.0).astype(np.float32)
+    th = prep.thermal_media_properties(med, np.ones(shape), T, 0.0, downsample=ds)
+    assert set(np.round(th["VHC"], 3)) == {3.9, 4.4}
