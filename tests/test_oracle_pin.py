@@ -54,6 +54,18 @@ def test_mc_oracle_matches_reference_golden(name, oracle_lib):
     assert ok, rep
 
 
+@pytest.mark.parametrize("name", sorted(mccases.FLUO_CASES))
+def test_fluorescence_oracle_matches_reference_golden(name, oracle_lib):
+    """Fluorescence runs (the reference MEX as simType 2): oracle batches vs the committed ones."""
+    from oracle import orc
+    with open(os.path.join(GOLD, "mc_ref_summaries.json")) as f:
+        golden = json.load(f)[name]
+    mc_in = mexargs.prepare_mc(mccases.FLUO_CASES[name](), 2)
+    ob = [mcstats.summaries(orc.oracle_mc(dict(mc_in, seed=1 + s), 0), mc_in) for s in range(K)]
+    ok, rep, worst = mcstats.ztest(golden, ob)
+    assert ok, rep
+
+
 def test_mc_oracle_deterministic(oracle_lib):
     from oracle import orc
     mc_in = mexargs.prepare_mc(mccases.c0_small())
