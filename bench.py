@@ -34,6 +34,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -74,7 +75,7 @@ class ClockSampler:
 
     def __init__(self, gpu_index=0):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")
+        self.path = os.path.join(tempfile.gettempdir(), "mcb_bench_clocks_%d.csv" % os.getpid())
         self.gpu = gpu_index
 
     def __enter__(self):
@@ -229,8 +230,8 @@ def run_ours(args):
                 "timing": "wall clock around mcb_heat_forward (host buffers)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": src,
-                     # DRAM bytes of one DG-ADI step (X + Y + Z pass) from the cold-cache ncu capture
-                     # (profiles/heat_dgadi_c1_100cube.md); in the timed loop the grid is L2-resident
+                     # DRAM bytes of one DG-ADI step (X + Y + Z pass) from a cold-cache ncu capture of
+                     # this workload; in the timed loop the grid is L2-resident
                      "traffic": HEAT_STEP_DRAM_BYTES, "traffic_note": "ncu cold-cache capture, bytes per DG-ADI step",
                      "algorithmic_bytes_per_voxel_update": bytes_per_update,
                      "kernel": "DG-ADI step (pass_x + pass_yz<y> + pass_yz<z>)"},

@@ -241,9 +241,10 @@ MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, cons
  * 66 bytes per voxel (58 without damage, 62 with damage but no light) plus 8 per sensor and
  * step (sensorTemps history) and small per-medium tables; larger problems return MCB_EINVAL
  * naming the limit. The context comes from mcb_ctx_create, which does allocate: create it
- * at set-up. The first call on a device performs set-up (cudaGetSymbolAddress of the scratch);
- * a caller that captures streams makes that first call before capture begins. There is one
- * scratch per device: calls that overlap in time on the same device race; serialise them. */
+ * at set-up. The first call on a device performs set-up (cudaGetSymbolAddress of the scratch).
+ * The call is synchronous (it waits for ctx's stream and reads its events before returning), so
+ * it must not be made while ctx's stream is being captured. There is one scratch per device:
+ * calls that overlap in time on the same device race; serialise them. */
 MCB_API mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_params *p, float *T, float *Omega,
                                            double *sensorTemps, float *maxMediaTemps);
 

@@ -212,32 +212,39 @@ class McModelBuffers:
         self.mc_in = mc_in
 
 
+def result_shapes(mc_in):
+    """MATLAB shapes of the tallied outputs of one MC call, as MCmatlab.c allocates them
+    (:461-493); every shape carries the wavelength as its last axis."""
+    nx, ny, nz = mc_in["nx"], mc_in["ny"], mc_in["nz"]
+    nL = np.asarray(mc_in["mua"]).shape[1]
+    bt = mc_in["boundaryType"]
+    sd = mc_in["sourceDistribution"] is not None
+    LC = mc_in["LC"]
+    nTB = 0 if sd else int(LC["nTimeBins"])
+    res = int(LC["res"])
+    shapes = {}
+    if mc_in["calcNFR"]:
+        shapes["NFR"] = (nx, ny, nz, nL)
+    if mc_in["useLightCollector"]:
+        shapes["image"] = (res, res, nTB + 2 if nTB else 1, nL)
+    ffr = int(mc_in["farFieldRes"])
+    if ffr:
+        shapes["farField"] = (ffr, ffr, nL)
+    if bt == 1:
+        shapes.update(NI_xpos=(ny, nz, nL), NI_xneg=(ny, nz, nL), NI_ypos=(nx, nz, nL),
+                      NI_yneg=(nx, nz, nL), NI_zpos=(nx, ny, nL), NI_zneg=(nx, ny, nL))
+    elif bt == 2:
+        shapes["NI_zneg"] = (KILLRANGE * nx, KILLRANGE * ny, nL)
+    elif bt == 3:
+        shapes.update(NI_zpos=(nx, ny, nL), NI_zneg=(nx, ny, nL))
+    return shapes
+
+
 class McResultBuffers:
     """Output arrays sized as MCmatlab.c allocates them (:461-493), returned in MATLAB shapes."""
 
     def __init__(self, mc_in, example_cap=0):
-        nx, ny, nz = mc_in["nx"], mc_in["ny"], mc_in["nz"]
-        nL = np.asarray(mc_in["mua"]).shape[1]
-        bt = mc_in["boundaryType"]
-        sd = mc_in["sourceDistribution"] is not None
-        LC = mc_in["LC"]
-        nTB = 0 if sd else int(LC["nTimeBins"])
-        res = int(LC["res"])
-        self.shapes = {}
-        if mc_in["calcNFR"]:
-            self.shapes["NFR"] = (nx, ny, nz, nL)
-        if mc_in["useLightCollector"]:
-            self.shapes["image"] = (res, res, nTB + 2 if nTB else 1, nL)
-        ffr = int(mc_in["farFieldRes"])
-        if ffr:
-            self.shapes["farField"] = (ffr, ffr, nL)
-        if bt == 1:
-            self.shapes.update(NI_xpos=(ny, nz, nL), NI_xneg=(ny, nz, nL), NI_ypos=(nx, nz, nL),
-                               NI_yneg=(nx, nz, nL), NI_zpos=(nx, ny, nL), NI_zneg=(nx, ny, nL))
-        elif bt == 2:
-            self.shapes["NI_zneg"] = (KILLRANGE * nx, KILLRANGE * ny, nL)
-        elif bt == 3:
-            self.shapes.update(NI_zpos=(nx, ny, nL), NI_zneg=(nx, ny, nL))
+        self.shapes = result_shapes(mc_in)
         self.arrays = {k: np.zeros(int(np.prod(s)), dtype=np.float32) for k, s in self.shapes.items()}
         r = mcb_mc_result()
         for k, a in self.arrays.items():

@@ -764,8 +764,9 @@ extern "C" double mcb_last_kernel_ms(const mcb_ctx *ctx) { return ctx ? ctx->las
 // There is one scratch per device. Calls that overlap in time on the same device (two host
 // threads, or two contexts on one device) share it and race; callers serialise them.
 // The first call on a device performs the set-up: it looks up the scratch's device address
-// with cudaGetSymbolAddress (which may load this file's module) and caches it; a caller that
-// captures streams makes that first call before capture begins.
+// with cudaGetSymbolAddress (which may load this file's module) and caches it.
+// The call is synchronous: it sums T on the host, then waits for ctx->stream and reads its
+// events before returning, so it must not be made while ctx->stream is being captured.
 // ---------------------------------------------------------------------------------------------
 namespace {
 constexpr size_t kHeatScratchBytes = (size_t)32 << 20;
@@ -844,6 +845,12 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
   if (!T || !maxMediaTemps) return set_error(ctx, MCB_EINVAL, "NULL T or maxMediaTemps");
   if (p->nSensors > 0 && !sensorTemps) return set_error(ctx, MCB_EINVAL, "sensorTemps is NULL");
   const bool damage = Omega != nullptr;
+  // the sensor history alone must fit before it is measured: 8 * nS * (steps + 1) could wrap
+  if (p->nSensors > 0 && (unsigned long long)p->steps + 1 > kHeatScratchBytes / (8 * (size_t)p->nSensors))
+    return set_error(ctx, MCB_EINVAL,
+                     "mcb_heat_forward_static: %d sensors over %d steps need more device scratch than its static "
+                     "limit of %zu bytes (8 bytes per sensor and step); use mcb_heat_forward",
+                     p->nSensors, p->steps, kHeatScratchBytes);
   mcb_heat_state s{};  // a view of the scratch; nothing in it is freed
   ScratchCarve measure{nullptr, 0};
   carve_static_state(measure, &s, p, damage);

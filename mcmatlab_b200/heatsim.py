@@ -22,6 +22,32 @@ import numpy as np
 from . import mexargs, native, prep
 
 
+def initial_max_media_temps(T, M_raw, nM):
+    """maxMediaTemps of a first heat run, one entry per unsplit medium present in the model
+    (simulateHeatDistribution.m:38-47). As in the reference, entry i (1-based) is the maximum of T
+    over the voxels whose raw medium index equals i, or -Inf where there is none."""
+    M_raw = np.asarray(M_raw)
+    T = np.asarray(T)
+    out = np.full(nM, -np.inf)
+    for i in range(1, nM + 1):
+        sel = M_raw == i
+        if sel.any():
+            out[i - 1] = float(T[sel].max())
+    return out
+
+
+def fold_max_media_temps(maxT, new, nBins):
+    """Folds the stepper's per-sub-medium maxima `new` into the per-medium maxima `maxT` in place:
+    medium iM takes the maximum over its sub-media iSM .. iSM + nBins[iM] - 1
+    (simulateHeatDistribution.m:268-272, :329-333, :390-394)."""
+    new = np.asarray(new, dtype=np.float64).ravel()
+    iSM = 0
+    for iM, nb in enumerate(nBins):
+        maxT[iM] = max(maxT[iM], float(new[iSM:iSM + nb].max()))
+        iSM += nb
+    return maxT
+
+
 def simulateHeatDistribution(model):
     G = model.G
     HS = model.HS
@@ -43,15 +69,8 @@ def simulateHeatDistribution(model):
     th = prep.thermal_media_properties(media, G.M_raw, T, fd_grid(), downsample=binning)
     HS.mediaProperties = {"name": th["names"], "VHC": th["VHC"], "TC": th["TC"], "A": th["A"], "E": th["E"]}
     HS.M = th["M"]
-    nM = len(th["VHC"])
     if first:
-        maxT = np.full(nM, -np.inf)
-        Mz = th["M"].astype(int) - 1
-        for i in range(nM):
-            sel = Mz == i
-            if sel.any():
-                maxT[i] = float(T[sel].max())
-        HS.maxMediaTemps = maxT
+        HS.maxMediaTemps = initial_max_media_temps(T, G.M_raw, len(th["nBins"]))
     damage = bool(np.any(th["A"]))
     if damage:
         if first or np.ndim(HS.Omega) == 0:
@@ -137,7 +156,7 @@ def simulateHeatDistribution(model):
             if built != generation:  # media recalculated: new media grid, coefficients and source
                 hp, built = params(lights, steps, dt), generation
             sens, mx = state.step(hp)
-            maxT[:] = np.maximum(maxT, mx.ravel().astype(np.float64))
+            fold_max_media_temps(maxT, mx, th["nBins"])
             if li is not None:
                 sensorTemps = sens if sensorTemps is None else np.concatenate([sensorTemps[:, :-1], sens], axis=1)
             if period > 0 and (first_idx + i + 1) % period == 0:

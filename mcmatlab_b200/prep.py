@@ -544,7 +544,7 @@ def thermal_media_properties(mediaList, M_raw, T=37.0, FD=0.0, downsample=None):
         E[iSM:iSM + nSM] = float(med.E)
         iSM += nSM
     return dict(VHC=VHC, TC=TC, A=A, E=E, M=np.asfortranarray(Msub.reshape(shape, order="F").astype(np.uint8)),
-                names=names)
+                names=names, nBins=[int(getattr(m, "nBins", 1)) for m in trimmed])
 
 
 def calc_dTdt_arrays(VHC, TC, dx, dy, dz, NA_sum, P, M1):

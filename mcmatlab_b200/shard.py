@@ -56,27 +56,35 @@ def _weights(mc_in, rank, world):
 
 def merge(out, mc_in, rank, world, allreduce):
     """Combines this rank's outputs with the other ranks' through `allreduce(flat float64 array)
-    -> summed array` (one call). Returns the merged output dict (on every rank)."""
+    -> summed array` (one call). Returns the merged output dict (on every rank).
+
+    The layout of the reduced buffer comes from mc_in alone (abi.result_shapes), so every rank
+    submits a buffer of the same length and order whatever its own run produced: an output this
+    rank lacks (a rank that ran no packets passes out=None) contributes zeros. Non-finite values
+    are reduced as they are, so a NaN on any rank stays NaN in the merge, as combineModels gives."""
+    from .abi import result_shapes
     w, nL = _weights(mc_in, rank, world)
-    keys, parts, shapes = [], [], []
-    for k in WEIGHTED:
+    shapes = result_shapes(mc_in)
+    keys = [k for k in WEIGHTED if k in shapes]
+    out = out if out is not None else {}
+    parts = []
+    for k in keys:
+        shp = shapes[k]
         a = out.get(k)
-        if a is None or np.size(a) <= 1 or not np.all(np.isfinite(a)):
+        if a is None or np.shape(a) != shp:
+            parts.append(np.zeros(int(np.prod(shp))))
             continue
         a = np.asarray(a, dtype=np.float64)
-        assert a.shape[-1] == nL, k  # every tallied output carries the wavelength as its last axis
-        scaled = a * w
-        keys.append(k)
-        shapes.append(a.shape)
-        parts.append(scaled.reshape(-1, order="F"))
-    counts = np.array([float(out["nPhotons"]), float(out["nPhotonsCollected"]), float(out["nThreads"])])
-    flat = np.concatenate(parts + [counts]) if parts else counts
-    total = allreduce(flat)
+        parts.append((a * w).reshape(-1, order="F"))
+    counts = np.array([float(out.get("nPhotons", 0.0)), float(out.get("nPhotonsCollected", 0.0)),
+                       float(out.get("nThreads", 0.0))])
+    total = allreduce(np.concatenate(parts + [counts]))
     res = dict(out)
     off = 0
-    for k, shp in zip(keys, shapes):
+    for k in keys:
+        shp = shapes[k]
         n = int(np.prod(shp))
-        res[k] = total[off:off + n].reshape(shp, order="F").astype(np.asarray(out[k]).dtype)
+        res[k] = total[off:off + n].reshape(shp, order="F").astype(np.float32)
         off += n
     res["nPhotons"] = total[off]
     res["nPhotonsCollected"] = total[off + 1]
@@ -106,5 +114,18 @@ def sharded_mc_run(mc_in, run=None, group=None):
         from . import native
         run = native.mc_run
     rank, world = dist.get_rank(group), dist.get_world_size(group)
-    out = run(shard_model(mc_in, rank, world))
-    return merge(out, mc_in, rank, world, torch_allreduce(group))
+    return sharded_run(mc_in, rank, world, run, torch_allreduce(group))
+
+
+def sharded_run(mc_in, rank, world, run, allreduce):
+    """One rank's part of a sharded run. Every check that can fail happens before any work and
+    gives the same answer on every rank (it depends on mc_in only), so no rank leaves while the
+    others wait in the collective. A rank whose shard is empty (fewer packets than ranks) runs
+    nothing and contributes zeros."""
+    total = float(mc_in["nPhotonsRequested"])
+    if not math.isfinite(total) or mc_in.get("requestCollectedPhotons"):
+        raise ValueError("sharding needs a fixed launched-packet count")
+    if int(total) < 1:
+        raise ValueError("nPhotonsRequested must be at least 1")
+    out = run(shard_model(mc_in, rank, world)) if shard_count(total, rank, world) > 0 else None
+    return merge(out, mc_in, rank, world, allreduce)

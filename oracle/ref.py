@@ -35,9 +35,9 @@ _NP = {6: np.float64, 7: np.float32, 9: np.uint8, 3: np.uint8, 12: np.int32, 13:
 
 def build(refsrc=None):
     """Builds oracle/_ref with the committed Makefile (needs the reference sources)."""
-    args = ["make", "-C", HERE, "all"]
+    args = ["make", "-C", HERE, "oracle"]
     if refsrc:
-        args.append("REFSRC=%s" % refsrc)
+        args += ["ref", "REFSRC=%s" % refsrc]
     subprocess.run(args, check=True, capture_output=True)
 
 

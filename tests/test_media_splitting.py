@@ -127,3 +127,28 @@ def test_scalar_property_functions_apply_elementwise(oracle_lib):
     T = np.where(np.arange(125).reshape(shape) % 2 == 0, 40.0, 60.0).astype(np.float32)
     th = prep.thermal_media_properties(med, np.ones(shape), T, 0.0, downsample=ds)
     assert set(np.round(th["VHC"], 3)) == {3.9, 4.4}
+
+
+def test_max_media_temps_fold_per_unsplit_medium(oracle_lib):
+    """maxMediaTemps keeps one entry per unsplit medium: the stepper's per-sub-medium maxima are
+    folded over each medium's nBins sub-media (simulateHeatDistribution.m:268-272), and the first
+    run starts from the maxima over the raw medium index (:38-47)."""
+    from mcmatlab_b200 import heatsim
+    rng = np.random.default_rng(4)
+    shape = (6, 5, 4)
+    M_raw = np.ones(shape)
+    M_raw[:, :, 2:] = 2
+    T = rng.uniform(30, 50, shape).astype(np.float32)
+    th_media = [mm.mediumProperties(name="a", VHC=3.9, TC=0.0037, nBins=3),
+                mm.mediumProperties(name="b", VHC=lambda T, FD: 3.0 + 0.01 * T, TC=0.005, nBins=4)]
+    th = prep.thermal_media_properties(th_media, M_raw, T, 0.0, downsample=_oracle_ds(oracle_lib))
+    assert th["nBins"] == [3, 4] and len(th["VHC"]) == 7
+    maxT = heatsim.initial_max_media_temps(T, M_raw, len(th["nBins"]))
+    assert maxT.shape == (2,)
+    assert maxT[0] == T[M_raw == 1].max() and maxT[1] == T[M_raw == 2].max()
+    new = np.array([10.0, 60.0, 20.0, 1.0, 2.0, 70.0, 3.0], dtype=np.float32)
+    heatsim.fold_max_media_temps(maxT, new, th["nBins"])
+    assert maxT[0] == 60.0 and maxT[1] == 70.0
+    low = np.zeros(7, dtype=np.float32)
+    heatsim.fold_max_media_temps(maxT, low, th["nBins"])
+    assert maxT[0] == 60.0 and maxT[1] == 70.0

@@ -77,3 +77,65 @@ def test_shards_run_disjoint_streams(oracle_lib):
     res = shard.merge(outs[1], mc_in, 1, 2, fake_allreduce(1))
     full = orc.oracle_mc(mc_in, 4)
     assert np.max(np.abs(res["NFR"] - full["NFR"])) <= 1e-5 * np.max(full["NFR"])
+
+
+def _rank_few(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import orc
+        m = _case()
+        m["nPhotonsRequested"] = 2.0
+        out = shard.sharded_mc_run(m, run=lambda mm: orc.oracle_mc(mm, 1))
+        q.put((rank, float(out["nPhotons"]), np.asarray(out["NFR"], np.float64)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_fewer_packets_than_ranks_merges_without_hanging(oracle_lib):
+    """Three gloo ranks share two packets: the rank with an empty shard runs nothing and
+    contributes zeros, every rank submits the same buffer layout, and all of them return the
+    unsharded two-packet result."""
+    from oracle import orc
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank_few, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(3)]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    m = _case()
+    m["nPhotonsRequested"] = 2.0
+    full = orc.oracle_mc(m, 1)
+    for rank, n, nfr in got:
+        assert n == 2.0
+        np.testing.assert_allclose(nfr, np.asarray(full["NFR"], np.float64), rtol=1e-5, atol=1e-6 * np.max(full["NFR"]))
+
+
+def test_empty_run_is_rejected_on_every_rank_before_the_collective():
+    calls = []
+    m = _case()
+    m["nPhotonsRequested"] = 0.0
+    for rank in range(2):
+        with pytest.raises(ValueError):
+            shard.sharded_run(m, rank, 2, run=lambda mm: calls.append(mm), allreduce=lambda a: calls.append(a))
+    assert calls == []
+
+
+def test_merge_layout_is_independent_of_the_rank_outputs():
+    """A rank whose run lacks an output, or holds NaNs, still submits the full layout."""
+    m = _case()
+    sizes = []
+
+    def fake(a):
+        sizes.append(a.size)
+        return a
+    shard.merge(None, m, 0, 2, fake)
+    shard.merge({"NFR": np.full((2, 2, 2, 1), np.nan), "nPhotons": 1.0, "nPhotonsCollected": 0.0, "nThreads": 1.0},
+                m, 1, 2, fake)
+    assert sizes[0] == sizes[1] and sizes[0] > 3

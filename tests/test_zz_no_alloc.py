@@ -58,12 +58,16 @@ def test_static_entry_allocates_no_device_memory():
 
 def test_static_entry_rejects_grids_beyond_its_scratch():
     from mcmatlab_b200 import native
-    big = heatcases._base(100, 5, 0, True, 1, 0.9, True)  # 1e6 voxels x 66 B > 32 MiB
+    big = heatcases._base(128, 5, 0, True, 1, 0.9, True)  # 2.1e6 voxels: beyond 32 MiB
     with pytest.raises(native.MCBError, match="static limit"):
-        native.heat_forward_static(big["T0"], big["Omega0"], big["hp"], 100, 100, 100)
+        native.heat_forward_static(big["T0"], big["Omega0"], big["hp"], 128, 128, 128)
+    # a small grid whose sensor history (8 B per sensor and step) alone exceeds the scratch
+    long = heatcases._base(8, 6, 0, True, 2_000_000, 0.9, False)
+    with pytest.raises(native.MCBError, match="static limit"):
+        native.heat_forward_static(long["T0"], None, long["hp"], 8, 8, 8)
     # the context stays usable, and the same grid runs through the allocating entry
     case = heatcases.CASES["insulated_on"]()
     nx, ny, nz = case["n"]
     ref = native.heat_forward(case["T0"], case["Omega0"], case["hp"], nx, ny, nz)
     _compare(ref, native.heat_forward_static(case["T0"], case["Omega0"], case["hp"], nx, ny, nz), case)
-    native.heat_forward(big["T0"], big["Omega0"], big["hp"], 100, 100, 100)
+    native.heat_forward(big["T0"], big["Omega0"], big["hp"], 128, 128, 128)
