@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmcb200.so")
-SOURCES = ["capi.cu", "mc_transport.cu", "heat_adi.cu", "heat_adjoint.cu", "normals.cu", "downsample.cu"]
+SOURCES = ["capi.cu", "mc_transport.cu", "heat_adi.cu", "heat_stream.cu", "heat_adjoint.cu", "normals.cu", "downsample.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-Xptxas", "-v", "--expt-relaxed-constexpr"]

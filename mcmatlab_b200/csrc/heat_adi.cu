@@ -450,10 +450,64 @@ void free_state_buffers(mcb_heat_state *s) {
   if (s->block) cudaFree(s->block);
   if (s->sens) cudaFree(s->sens);
   if (s->sIdx) cudaFree(s->sIdx);
+  delete s->maps;
+  s->maps = nullptr;
   s->block = nullptr;
   s->sens = s->sIdx = nullptr;
   s->sensCap = 0;
   s->sCap = 0;
+  s->streamed = false;
+}
+
+// Streamed state (heat_stream.cu) for p's grid in one allocation, with its TMA descriptors.
+mcb_status stream_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
+  free_state_buffers(s);
+  size_t need = 0;
+  mcb_heat_state probe{};
+  stream_carve([&](size_t b) { need += (b + 255) & ~(size_t)255; return (void *)nullptr; }, &probe, p, damage, true);
+  MCB_CUDA(ctx, cudaMalloc(&s->block, need));
+  char *cur = (char *)s->block;
+  stream_carve([&](size_t b) { char *q = cur; cur += (b + 255) & ~(size_t)255; return (void *)q; }, s, p, damage, true);
+  s->streamed = true;
+  s->nx = p->nx;
+  s->ny = p->ny;
+  s->nz = p->nz;
+  s->nM = p->nM;
+  s->L = (long long)p->nx * p->ny * p->nz;
+  s->damage = damage;
+  s->maps = new StreamMaps();
+  return stream_maps(ctx, s);
+}
+
+// Grow-only device buffers of the sensor inputs and history; uploads the sensor inputs.
+mcb_status sensor_buffers(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p) {
+  const int nS = p->nSensors;
+  const long long nt = p->steps;
+  if (nS <= 0) return MCB_OK;
+  if (s->sCap < nS) {
+    if (s->sIdx) cudaFree(s->sIdx);
+    s->sIdx = nullptr;
+    s->sCap = 0;
+    MCB_CUDA(ctx, cudaMalloc(&s->sIdx, 32 * (size_t)nS));
+    s->sW = s->sIdx + nS;
+    s->sCap = nS;
+  }
+  if (s->sensCap < (long long)nS * (nt + 1)) {
+    if (s->sens) cudaFree(s->sens);
+    s->sens = nullptr;
+    s->sensCap = 0;
+    MCB_CUDA(ctx, cudaMalloc(&s->sens, 8 * (size_t)nS * (nt + 1)));
+    s->sensCap = (long long)nS * (nt + 1);
+  }
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->sIdx, p->tempSensorCornerIdxs, 8 * (size_t)nS, cudaMemcpyHostToDevice, ctx->stream));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, ctx->stream));
+  return MCB_OK;
+}
+
+// Whether a state of the right kind and shape for p exists.
+bool state_fits(const mcb_heat_state *s, const mcb_heat_params *p, bool damage, bool streamed) {
+  return s->block && s->streamed == streamed && s->nx == p->nx && s->ny == p->ny && s->nz == p->nz && s->nM == p->nM &&
+         s->damage == damage;
 }
 
 mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
@@ -497,15 +551,7 @@ mcb_status state_alloc(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   return MCB_OK;
 }
 
-// Per medium {x0, E/R} with x0 = log A - E / (R T0), T0 = base temperature in kelvin (FP64 on the
-// host); E/R = 0 marks media without damage.
-void damage_table(const mcb_heat_params *p, double base, float2 *out) {
-  const double T0 = base + kCelsiusZero;
-  for (int m = 0; m < p->nM; m++) {
-    const double c1 = p->E[m] / kGasR;
-    out[m] = p->E[m] != 0.0 ? make_float2((float)(std::log(p->A[m]) - c1 / T0), (float)c1) : make_float2(0.f, 0.f);
-  }
-}
+void damage_table(const mcb_heat_params *p, double base, float2 *out) { heat_damage_table(p, base, out); }
 
 // Uploads the media/coefficients/source of p and the state T, Omega (host pointers).
 mcb_status state_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T, const float *Omega) {
@@ -552,21 +598,7 @@ mcb_status state_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p,
   cudaStream_t st = ctx->stream;
   const long long nt = p->steps;
   const int nS = p->nSensors;
-  if (nS > 0) {
-    if (s->sCap < nS) {
-      if (s->sIdx) cudaFree(s->sIdx);
-      MCB_CUDA(ctx, cudaMalloc(&s->sIdx, 32 * (size_t)nS));
-      s->sW = s->sIdx + nS;
-      s->sCap = nS;
-    }
-    if (s->sensCap < (long long)nS * (nt + 1)) {
-      if (s->sens) cudaFree(s->sens);
-      MCB_CUDA(ctx, cudaMalloc(&s->sens, 8 * (size_t)nS * (nt + 1)));
-      s->sensCap = (long long)nS * (nt + 1);
-    }
-    MCB_CUDA(ctx, cudaMemcpyAsync(s->sIdx, p->tempSensorCornerIdxs, 8 * (size_t)nS, cudaMemcpyHostToDevice, st));
-    MCB_CUDA(ctx, cudaMemcpyAsync(s->sW, p->tempSensorInterpWeights, 24 * (size_t)nS, cudaMemcpyHostToDevice, st));
-  }
+  MCB_TRY(sensor_buffers(ctx, s, p));
   if (p->lightsOn && p->dTdt_abs == nullptr) return set_error(ctx, MCB_EINVAL, "dTdt_abs missing while lightsOn");
   HeatStepper ks;
   MCB_TRY(heat_stepper(ctx, s, p, &ks));
@@ -617,13 +649,22 @@ mcb_status state_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Omeg
 
 namespace mcb {
 
+// Per medium {x0, E/R} with x0 = log A - E / (R T0), T0 = base temperature in kelvin (FP64 on the
+// host); E/R = 0 marks media without damage.
+void heat_damage_table(const mcb_heat_params *p, double base, float2 *out) {
+  const double T0 = base + kCelsiusZero;
+  for (int m = 0; m < p->nM; m++) {
+    const double c1 = p->E[m] / kGasR;
+    out[m] = p->E[m] != 0.0 ? make_float2((float)(std::log(p->A[m]) - c1 / T0), (float)c1) : make_float2(0.f, 0.f);
+  }
+}
+
 mcb_status heat_check_params(mcb_ctx *ctx, const mcb_heat_params *p) { return check_params(ctx, p); }
 
 mcb_status heat_state_init(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T,
                            const float *Omega) {
   const bool damage = Omega != nullptr;
-  if (!s->block || s->nx != p->nx || s->ny != p->ny || s->nz != p->nz || s->nM != p->nM || s->damage != damage)
-    MCB_TRY(state_alloc(ctx, s, p, damage));
+  if (!state_fits(s, p, damage, false)) MCB_TRY(state_alloc(ctx, s, p, damage));
   return state_upload(ctx, s, p, T, Omega);
 }
 
@@ -677,7 +718,7 @@ extern "C" mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, f
   if (!T || !maxMediaTemps) return set_error(ctx, MCB_EINVAL, "NULL T or maxMediaTemps");
   if (p->nSensors > 0 && !sensorTemps) return set_error(ctx, MCB_EINVAL, "sensorTemps is NULL");
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
-  // the context keeps one state; it is reallocated when the grid or damage setting changes
+  // the context keeps one state; it is reallocated when the grid, its kind or the damage setting changes
   mcb_heat_state *s = ctx->heat;
   const bool damage = Omega != nullptr;
   if (!s) {
@@ -685,8 +726,15 @@ extern "C" mcb_status mcb_heat_forward(mcb_ctx *ctx, const mcb_heat_params *p, f
     s->ctx = ctx;
     ctx->heat = s;
   }
-  if (!s->block || s->nx != p->nx || s->ny != p->ny || s->nz != p->nz || s->nM != p->nM || s->damage != damage)
-    MCB_TRY(state_alloc(ctx, s, p, damage));
+  if (stream_supported(p->nx, p->ny, p->nz)) {
+    if (!state_fits(s, p, damage, true)) MCB_TRY(stream_alloc(ctx, s, p, damage));
+    MCB_TRY(stream_upload(ctx, s, p, T, Omega));
+    if (p->lightsOn) MCB_TRY(stream_upload_q(ctx, s, p->dTdt_abs));
+    MCB_TRY(sensor_buffers(ctx, s, p));
+    MCB_TRY(stream_step(ctx, s, p, s->sens, sensorTemps, maxMediaTemps, true));
+    return stream_download(ctx, s, T, Omega);
+  }
+  if (!state_fits(s, p, damage, false)) MCB_TRY(state_alloc(ctx, s, p, damage));
   MCB_TRY(state_upload(ctx, s, p, T, Omega));
   MCB_TRY(state_step(ctx, s, p, sensorTemps, maxMediaTemps));
   return state_download(ctx, s, T, Omega);
@@ -701,8 +749,15 @@ extern "C" mcb_status mcb_heat_state_create(mcb_ctx *ctx, const mcb_heat_params 
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
   mcb_heat_state *s = new mcb_heat_state();
   s->ctx = ctx;
-  mcb_status st = state_alloc(ctx, s, p, Omega != nullptr);
-  if (st == MCB_OK) st = state_upload(ctx, s, p, T, Omega);
+  mcb_status st;
+  if (stream_supported(p->nx, p->ny, p->nz)) {
+    st = stream_alloc(ctx, s, p, Omega != nullptr);
+    if (st == MCB_OK) st = stream_upload(ctx, s, p, T, Omega);
+    if (st == MCB_OK && p->lightsOn) st = stream_upload_q(ctx, s, p->dTdt_abs);
+  } else {
+    st = state_alloc(ctx, s, p, Omega != nullptr);
+    if (st == MCB_OK) st = state_upload(ctx, s, p, T, Omega);
+  }
   if (st != MCB_OK) {
     free_state_buffers(s);
     delete s;
@@ -722,6 +777,11 @@ extern "C" mcb_status mcb_heat_state_step(mcb_heat_state *s, const mcb_heat_para
     return set_error(ctx, MCB_EINVAL, "parameters do not match the state's grid");
   if (p->nSensors > 0 && !sensorTemps) return set_error(ctx, MCB_EINVAL, "sensorTemps is NULL");
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (s->streamed) {
+    if (p->lightsOn && p->dTdt_abs) MCB_TRY(stream_upload_q(ctx, s, p->dTdt_abs));
+    MCB_TRY(sensor_buffers(ctx, s, p));
+    return stream_step(ctx, s, p, s->sens, sensorTemps, maxMediaTemps, true);
+  }
   if (p->lightsOn && p->dTdt_abs)
     MCB_CUDA(ctx, cudaMemcpyAsync(s->Q, p->dTdt_abs, 4 * s->L, cudaMemcpyHostToDevice, ctx->stream));
   return state_step(ctx, s, p, sensorTemps, maxMediaTemps);
@@ -731,6 +791,7 @@ extern "C" mcb_status mcb_heat_state_read(mcb_heat_state *s, float *T, float *Om
   using namespace mcb;
   if (!s) return MCB_EINVAL;
   MCB_CUDA(s->ctx, cudaSetDevice(s->ctx->device));
+  if (s->streamed) return stream_download(s->ctx, s, T, Omega);
   return state_download(s->ctx, s, T, Omega);
 }
 
@@ -809,7 +870,17 @@ struct ScratchCarve {
   }
 };
 
-// Lays the stepper's buffers out in the scratch (or measures them when c.base is null).
+// Lays the streamed stepper's buffers and the sensor arrays out in the scratch (or measures
+// them when c.base is null).
+void carve_static_stream(ScratchCarve &c, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
+  const int nS = p->nSensors;
+  stream_carve([&](size_t b) { return c.take(b); }, s, p, damage, p->lightsOn != 0);
+  s->sIdx = nS ? (double *)c.take(8 * (size_t)nS) : nullptr;
+  s->sW = nS ? (double *)c.take(24 * (size_t)nS) : nullptr;
+  s->sens = nS ? (double *)c.take(8 * (size_t)nS * (size_t)(p->steps + 1)) : nullptr;
+}
+
+// Lays the factored stepper's buffers out in the scratch (or measures them when c.base is null).
 void carve_static_state(ScratchCarve &c, mcb_heat_state *s, const mcb_heat_params *p, bool damage) {
   const long long L = (long long)p->nx * p->ny * p->nz;
   const int nM = p->nM, nS = p->nSensors;
@@ -852,17 +923,43 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
                      "limit of %zu bytes (8 bytes per sensor and step); use mcb_heat_forward",
                      p->nSensors, p->steps, kHeatScratchBytes);
   mcb_heat_state s{};  // a view of the scratch; nothing in it is freed
+  const bool streamed = stream_supported(p->nx, p->ny, p->nz);
   ScratchCarve measure{nullptr, 0};
-  carve_static_state(measure, &s, p, damage);
+  if (streamed) carve_static_stream(measure, &s, p, damage);
+  else carve_static_state(measure, &s, p, damage);
   if (measure.used > kHeatScratchBytes)
     return set_error(ctx, MCB_EINVAL,
                      "mcb_heat_forward_static: this grid needs %zu bytes of device scratch, more than its static "
-                     "limit of %zu bytes (about 66 bytes per voxel plus 8 per sensor and step); use mcb_heat_forward",
+                     "limit of %zu bytes (about 22 bytes per voxel, 30 with damage, of the x-padded grid, plus 8 per "
+                     "sensor and step); use mcb_heat_forward",
                      measure.used, kHeatScratchBytes);
   MCB_CUDA(ctx, cudaSetDevice(ctx->device));
   void *base = nullptr;
   MCB_TRY(heat_scratch(ctx, &base));
   ScratchCarve carve{(char *)base, 0};
+  if (streamed) {
+    carve_static_stream(carve, &s, p, damage);
+    StreamMaps maps;  // on the stack: the descriptors only live for this call
+    s.maps = &maps;
+    s.ctx = ctx;
+    s.streamed = true;
+    mcb_status rc = stream_maps(ctx, &s);
+    if (rc == MCB_OK) rc = stream_upload(ctx, &s, p, T, Omega);
+    if (rc == MCB_OK && p->lightsOn) rc = stream_upload_q(ctx, &s, p->dTdt_abs);
+    if (rc == MCB_OK && p->nSensors) {
+      const cudaError_t e1 = cudaMemcpyAsync(s.sIdx, p->tempSensorCornerIdxs, 8 * (size_t)p->nSensors,
+                                             cudaMemcpyHostToDevice, ctx->stream);
+      const cudaError_t e2 = cudaMemcpyAsync(s.sW, p->tempSensorInterpWeights, 24 * (size_t)p->nSensors,
+                                             cudaMemcpyHostToDevice, ctx->stream);
+      if (e1 != cudaSuccess || e2 != cudaSuccess)
+        rc = set_error(ctx, MCB_ECUDA, "mcb_heat_forward_static: sensor upload failed");
+    }
+    // plain launches per step: instantiating a CUDA graph may allocate
+    if (rc == MCB_OK) rc = stream_step(ctx, &s, p, s.sens, sensorTemps, maxMediaTemps, false);
+    if (rc == MCB_OK) rc = stream_download(ctx, &s, T, Omega);
+    s.maps = nullptr;
+    return rc;
+  }
   carve_static_state(carve, &s, p, damage);
   s.ctx = ctx;
   s.nx = p->nx;

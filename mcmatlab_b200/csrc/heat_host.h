@@ -1,11 +1,42 @@
 // Host-side internals of the heat stepper shared by the forward entries (heat_adi.cu) and the
 // adjoint (heat_adjoint.cu): the device-resident state and the stepping set-up.
 #pragma once
+#include <cuda.h>
+
+#include <functional>
+
 #include "heat_common.cuh"
 #include "internal.h"
 
-// Device-resident stepper state: grids stay in HBM across calls.
+namespace mcb {
+// Grid shape of the streamed stepper: every grid is stored with an x pitch px >= nx (a multiple
+// of 16 that holds whole lane chunks of the X pass) so that every row starts on a TMA-aligned
+// boundary.
+struct StreamShape {
+  int nx = 0, ny = 0, nz = 0, px = 0;
+  long long Lp = 0;  // px * ny * nz
+};
+// TMA descriptors of the streamed stepper's tiles over this state's buffers.
+struct StreamMaps {
+  CUtensorMap xTh, xTr, xQr, xMh, xCr;  // X pass: T with y halo rows, T rows, Q rows, media with halo, codes
+  CUtensorMap yA, yM;                   // Y pass: A and media, 16 columns x whole y lines
+  CUtensorMap zA, zM, zT;               // Z pass: A, media and T, 16 columns x whole z lines
+};
+}  // namespace mcb
+
+// Device-resident stepper state: grids stay in HBM across calls. A state is either streamed
+// (heat_stream.cu: pitched grids, no stored factorisation) or factored (heat_adi.cu: dense grids
+// with the line factorisation stored per voxel, used by the adjoint and for axes over 512).
 struct mcb_heat_state {
+  bool streamed = false;
+  mcb::StreamShape shape;
+  mcb::StreamMaps *maps = nullptr;
+  uint8_t *code = nullptr;
+  float *H = nullptr;
+  float4 *Hd = nullptr;
+  int codeHs = -1;
+  bool qValid = false;
+  int lastW = 0;
   mcb_ctx *ctx = nullptr;
   int nx = 0, ny = 0, nz = 0, nM = 0;
   long long L = 0;
@@ -48,5 +79,20 @@ void heat_state_release(mcb_heat_state *s);
 mcb_status heat_stepper(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, HeatStepper *out);
 // Enqueues one step.
 void heat_step_launch(const HeatStepper &k, cudaStream_t st);
+// Per medium {x0, E/R} with x0 = log A - E / (R T0), T0 = base temperature in kelvin.
+void heat_damage_table(const mcb_heat_params *p, double base, float2 *out);
+
+// Streamed stepper (heat_stream.cu).
+bool stream_supported(int nx, int ny, int nz);
+StreamShape stream_shape(int nx, int ny, int nz);
+int stream_warmup(const float *c, float hdt, int nM);
+void stream_carve(const std::function<void *(size_t)> &take, mcb_heat_state *s, const mcb_heat_params *p, bool damage,
+                  bool withQ);
+mcb_status stream_maps(mcb_ctx *ctx, mcb_heat_state *s);
+mcb_status stream_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T, const float *Omega);
+mcb_status stream_upload_q(mcb_ctx *ctx, mcb_heat_state *s, const float *Q);
+mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, double *sensorTemps,
+                       float *maxMediaTemps, bool graphs);
+mcb_status stream_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Omega);
 
 }  // namespace mcb

@@ -1,0 +1,1013 @@
+// Streamed DG-ADI stepper for sm_100a: the forward heat path of mcb_heat_forward and
+// mcb_heat_state_* (replacing +MCmatlab/src/finiteElementHeatPropagator.c:688-821) for grids
+// whose axes are at most 512 voxels long.
+//
+// One time step of the reference is six grid passes (substep1a..3b, :249-647). Here it is three
+// streaming passes, one per direction, and nothing per voxel is stored besides the state:
+//   X pass: explicit stencil of the whole step on T^n (1a, and the half-corrections 2a, 3a),
+//           solve along x (1b); writes A1 - S_y with S_y = dt/2 D_y T^n.
+//   Y pass: solve along y (2b) on A1 - S_y; writes A2.
+//   Z pass: forms S_z = dt/2 D_z T^n from the T^n tile (3a), solves along z on A2 - S_z (3b),
+//           adds the Arrhenius damage with the mid-step temperature and the per-medium running
+//           maxima, and writes T^{n+1} in place.
+// Per voxel and step the passes move 38 bytes of DRAM traffic (X: T, Q, medium, neighbourhood
+// code in, A out; Y: A and medium in, A out; Z: A, T and medium in, T out) plus the damage
+// increment where damage accumulates.
+//
+// Tiles are staged in shared memory with TMA (cp.async.bulk.tensor, a two-stage mbarrier
+// pipeline in persistent blocks; X tiles are 8 x-lines with their y halo rows and the z
+// neighbour rows, Y and Z tiles 16 columns of whole lines, 64-byte swizzled), and the Y and Z
+// results leave through TMA stores. f32 grids are described to TMA as pairs (8-byte elements) and
+// byte grids as quads, so one box spans a whole x row of up to 512 voxels.
+//
+// Line coefficients are formed on the fly from the media and the per-call table
+// H(d, mi, mj) = dt/2 c(mi, mj, d) (substep1b builds its diagonal the same way, :326-349), and so
+// are the LU pivots b'_i = b_i - a_i c_{i-1} / b'_{i-1} of each line: a lane that owns the chunk
+// [s, e) of a line starts the pivot recurrence W rows before s from b'_{s-W} := b_{s-W}. The map
+// b -> b_i - a_i c_{i-1} / b is increasing, so the started value stays above the true pivot, and its
+// relative error shrinks by at most rho = max a c / (1 + a + c) per row (a = H(q, p), c = H(p, q)
+// over medium pairs; this uses b'_j >= 1 + c_j, which holds for these diagonally dominant rows).
+// The host picks W with rho^W <= 2^-26, below FP32 rounding; where rho >= 1 no bound holds and
+// every lane starts at row 0, which is the serial recurrence itself. Each line is then solved by
+// a warp (X) or a 16-lane group (Y, Z) as two chunked affine scans (forward elimination, back
+// substitution) in registers.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "heat_host.h"
+#include "tma.cuh"
+
+namespace mcb {
+
+namespace {
+
+constexpr int kXL = 8;  // x-lines per X tile, one warp each
+constexpr int kTW = 16;  // columns per Y/Z tile
+constexpr int kCodeSink = 64;
+
+// Shared-memory layout of one X-tile stage (byte offsets): T rows y0-1..y0+8 of plane z, T rows
+// y0..y0+7 of planes z-1 and z+1, Q rows, medium rows y0-1..y0+8, code rows.
+struct XLayout {
+  int offTm, offTp, offQ, offM, offC, stage;
+  uint32_t tx;
+};
+
+__host__ __device__ inline int up128(int b) { return (b + 127) & ~127; }
+
+__host__ __device__ inline XLayout x_layout(int px, bool q) {
+  XLayout L;
+  const int rowF = 4 * px;
+  L.offTm = up128((kXL + 2) * rowF);
+  L.offTp = L.offTm + up128(kXL * rowF);
+  L.offQ = L.offTp + up128(kXL * rowF);
+  L.offM = L.offQ + (q ? up128(kXL * rowF) : 0);
+  L.offC = L.offM + up128((kXL + 2) * px);
+  const int end = L.offC + up128(kXL * px);
+  L.stage = (end + 1023) & ~1023;
+  L.tx = (uint32_t)((kXL + 2) * rowF + 2 * kXL * rowF + (q ? kXL * rowF : 0) + (kXL + 2) * px + kXL * px);
+  return L;
+}
+
+// One Y/Z tile: nb boxes of BN rows (BN a multiple of 16, <= 256) of 16 columns; f32 tiles are
+// 64-byte swizzled rows, the medium tile plain 16-byte rows.
+struct YZLayout {
+  int nb, BN, offM, offT, stage;
+  uint32_t tx;
+};
+
+__host__ __device__ inline YZLayout yz_layout(int n, bool zpass) {
+  YZLayout L;
+  L.nb = n > 256 ? 2 : 1;
+  L.BN = (((n + L.nb - 1) / L.nb) + 15) & ~15;
+  const int rows = L.nb * L.BN;
+  L.offM = rows * 64;
+  L.offT = L.offM + ((rows * 16 + 1023) & ~1023);
+  L.stage = L.offT + (zpass ? rows * 64 : 0);
+  L.tx = (uint32_t)(rows * (64 + 16 + (zpass ? 64 : 0)));
+  return L;
+}
+
+// Byte offset of element (row i, column j) of a 64-byte-swizzled f32 tile (TMA SWIZZLE_64B:
+// address bits 4-5 are XORed with bits 7-8).
+__device__ __forceinline__ int swz(int i, int j) { return i * 64 + ((((j >> 2) ^ (i >> 1)) & 3) << 4) + ((j & 3) << 2); }
+
+}  // namespace
+
+struct StreamDev {
+  int nx, ny, nz, nM, px, W;
+  long long sxy;  // px * ny
+  float *T, *A;
+  const uint8_t *M, *code;
+  const float *Q;     // or nullptr (light off)
+  float *dOmega;      // or nullptr
+  const float *H;     // [3][nM][nM]: H[d*nM*nM + mj*nM + mi] = dt/2 c(mi, mj, d)
+  const float4 *Hd;   // [nM] diagonal {H(m,m,0), H(m,m,1), H(m,m,2), 0}
+  const float2 *dmg;  // [nM] Arrhenius exponent about the base temperature
+  float T0, dt;
+  unsigned int *maxEnc;
+  int hs;
+  double base;
+  int nS;
+  const double *sIdx, *sW;
+  double *sens;
+  int *stepCounter;
+  int *err;
+};
+
+namespace {
+
+// First 1024-byte boundary at or after p in shared memory (the swizzle pattern of the Y/Z tiles
+// is a function of the address bits, so tiles start on such a boundary; the dynamic allocation
+// carries 1 KB of slack for it).
+__device__ __forceinline__ unsigned char *align1024(unsigned char *p) {
+  const uint32_t a = smem_addr(p);
+  return p + (((a + 1023u) & ~1023u) - a);
+}
+
+// Correctly rounded reciprocal: the pivots' rounding enters every step of long runs.
+__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
+
+__device__ __forceinline__ float hcoef(const StreamDev &h, int d, int mi, int mj) {
+  return __ldg(h.H + (d * h.nM + mj) * h.nM + mi);
+}
+
+// Sensor interpolation (recordTempSensors, finiteElementHeatPropagator.c:652-664) on the pitched
+// state; sensor corner indices are dense 0-based linear indices.
+__device__ void record_sensors_p(const StreamDev &h, int col) {
+  for (int j = threadIdx.x; j < h.nS; j += blockDim.x) {
+    const long long li = (long long)h.sIdx[j];
+    const long long nxy = (long long)h.nx * h.ny;
+    const long long iz = li / nxy, r = li - iz * nxy, iy = r / h.nx, ix = r - iy * h.nx;
+    const long long i = ix + iy * h.px + iz * h.sxy, sx = 1, sy = h.px, sz = h.sxy;
+    const double wx = h.sW[j], wy = h.sW[j + h.nS], wz = h.sW[j + 2 * h.nS];
+    auto T = [&](long long k) { return (double)h.T[k] + h.base; };
+    h.sens[j + (long long)col * h.nS] =
+        (1 - wx) * (1 - wy) * (1 - wz) * T(i) + (1 - wx) * (1 - wy) * wz * T(i + sz) + (1 - wx) * wy * (1 - wz) * T(i + sy) +
+        (1 - wx) * wy * wz * T(i + sy + sz) + wx * (1 - wy) * (1 - wz) * T(i + sx) + wx * (1 - wy) * wz * T(i + sx + sz) +
+        wx * wy * (1 - wz) * T(i + sx + sy) + wx * wy * wz * T(i + sx + sy + sz);
+  }
+}
+
+// Chunked two-scan solve of one line whose lanes hold K consecutive rows each (G lanes per line,
+// an aligned sub-warp group): r (right-hand side in, solution out), fm = a_i / b'_{i-1},
+// bm = c_i / b'_i, ib = 1 / b'_i. Register slots past a lane's rows (a lane may hold fewer than K
+// rows, also in the middle of a line) are identity maps of both scans: fm = bm = 1, ib = r = 0.
+template <int K, int G>
+__device__ __forceinline__ void chunk_solve(float (&r)[K], const float (&fm)[K], const float (&bm)[K], const float (&ib)[K],
+                                            int g) {
+  float A = 0.f, B = 1.f;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    A = fmaf(fm[k], A, r[k]);
+    B *= fm[k];
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Au = __shfl_up_sync(0xffffffffu, A, off, G);
+    const float Bu = __shfl_up_sync(0xffffffffu, B, off, G);
+    if (g >= off) {
+      A = fmaf(B, Au, A);
+      B *= Bu;
+    }
+  }
+  float d = __shfl_up_sync(0xffffffffu, A, 1, G);
+  if (g == 0) d = 0.f;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    d = fmaf(fm[k], d, r[k]);
+    r[k] = d * ib[k];
+  }
+  A = 0.f;
+  B = 1.f;
+#pragma unroll
+  for (int k = K - 1; k >= 0; k--) {
+    A = fmaf(bm[k], A, r[k]);
+    B *= bm[k];
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Ad = __shfl_down_sync(0xffffffffu, A, off, G);
+    const float Bd = __shfl_down_sync(0xffffffffu, B, off, G);
+    if (g + off < G) {
+      A = fmaf(B, Ad, A);
+      B *= Bd;
+    }
+  }
+  float t = __shfl_down_sync(0xffffffffu, A, 1, G);
+  if (g == G - 1) t = 0.f;
+#pragma unroll
+  for (int k = K - 1; k >= 0; k--) {
+    t = fmaf(bm[k], t, r[k]);
+    r[k] = t;
+  }
+}
+
+// Pivots of a lane's `count` rows from their coefficients a[k], c[k] (rows s+k), given the
+// started pivot of row s-1 (bp, its coupling cprev; bp = 0 for s = 0); the remaining slots become
+// identity maps (chunk_solve).
+template <int K>
+__device__ __forceinline__ void lane_pivots(const float (&a)[K], const float (&c)[K], float bp, float cprev, int count,
+                                            float (&fm)[K], float (&bm)[K], float (&ib)[K]) {
+  float ibp = bp > 0.f ? frcp(bp) : 0.f;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    if (k < count) {
+      const float b = fmaf(-a[k] * cprev, ibp, 1.f + a[k] + c[k]);
+      ib[k] = frcp(b);
+      fm[k] = a[k] * ibp;
+      bm[k] = c[k] * ib[k];
+      ibp = ib[k];
+      cprev = c[k];
+    } else {
+      fm[k] = bm[k] = 1.f;
+      ib[k] = 0.f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// X pass
+// ---------------------------------------------------------------------------------------------
+
+template <int K>
+__device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, const XLayout &lay, int l, int y, int z, int lane) {
+  const int nx = h.nx, px = h.px;
+  const float *Tc = reinterpret_cast<const float *>(b) + (l + 1) * px;
+  float *rowA = reinterpret_cast<float *>(b + lay.offTm) + l * px;  // z-1 row, then the line's a_i
+  float *rowC = reinterpret_cast<float *>(b + lay.offTp) + l * px;  // z+1 row, then the line's c_i
+  const float *Qr = h.Q ? reinterpret_cast<const float *>(b + lay.offQ) + l * px : nullptr;
+  const uint8_t *Mc = b + lay.offM + (l + 1) * px;
+  const uint8_t *Cr = b + lay.offC + l * px;
+  const int s = lane * K;
+  const long long rowBase = (long long)y * px + (long long)z * h.sxy;
+  float r[K], sy[K], ca[K], cc[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) r[k] = sy[k] = ca[k] = cc[k] = 0.f;
+  const bool act = s < nx;
+  if (act) {
+    float tprev = s > 0 ? Tc[s - 1] : 0.f;
+#pragma unroll
+    for (int k4 = 0; k4 < K / 4; k4++) {
+      const int x4 = s + 4 * k4;
+      const float4 t4 = *reinterpret_cast<const float4 *>(Tc + x4);
+      const float4 ym4 = *reinterpret_cast<const float4 *>(Tc - px + x4);
+      const float4 yp4 = *reinterpret_cast<const float4 *>(Tc + px + x4);
+      const float4 zm4 = *reinterpret_cast<const float4 *>(rowA + x4);
+      const float4 zp4 = *reinterpret_cast<const float4 *>(rowC + x4);
+      const float4 q4 = Qr ? *reinterpret_cast<const float4 *>(Qr + x4) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float tnext = x4 + 4 < nx ? Tc[x4 + 4] : 0.f;
+      const uint32_t m4 = *reinterpret_cast<const uint32_t *>(Mc + x4);
+      const uint32_t c4 = *reinterpret_cast<const uint32_t *>(Cr + x4);
+      const float tv[4] = {t4.x, t4.y, t4.z, t4.w}, ymv[4] = {ym4.x, ym4.y, ym4.z, ym4.w},
+                  ypv[4] = {yp4.x, yp4.y, yp4.z, yp4.w}, zmv[4] = {zm4.x, zm4.y, zm4.z, zm4.w},
+                  zpv[4] = {zp4.x, zp4.y, zp4.z, zp4.w}, qv[4] = {q4.x, q4.y, q4.z, q4.w};
+      float av[4], cv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int k = 4 * k4 + u, x = x4 + u;
+        const float t = tv[u];
+        const float tL = u ? tv[u - 1] : tprev;
+        const float tR = u < 3 ? tv[u + 1] : tnext;
+        const int m = (m4 >> (8 * u)) & 255, code = (c4 >> (8 * u)) & 255;
+        float a = 0.f, c = 0.f, dy = 0.f, dz = 0.f, rr = 0.f;
+        if (x < nx) {
+          rr = t;
+          if (!(code & kCodeSink)) {
+            if ((code & 63) == 0) {
+              const float4 H = __ldg(h.Hd + m);
+              a = c = H.x;
+              dy = H.y * ((ymv[u] - t) + (ypv[u] - t));
+              dz = H.z * ((zmv[u] - t) + (zpv[u] - t));
+            } else {
+              // a neighbour is missing or of another medium: every face looked up
+              if (x > 0) a = hcoef(h, 0, m, Mc[x - 1]);
+              if (x < nx - 1) c = hcoef(h, 0, m, Mc[x + 1]);
+              if (y > 0) dy += hcoef(h, 1, m, Mc[x - px]) * (ymv[u] - t);
+              if (y < h.ny - 1) dy += hcoef(h, 1, m, Mc[x + px]) * (ypv[u] - t);
+              const long long p = rowBase + x;
+              if (z > 0) dz += hcoef(h, 2, m, h.M[p - h.sxy]) * (zmv[u] - t);
+              if (z < h.nz - 1) dz += hcoef(h, 2, m, h.M[p + h.sxy]) * (zpv[u] - t);
+            }
+            // rhs of 1a: T + dt (Q + D_y T + D_z T) + dt/2 D_x T, with dt D_y T = 2 S_y
+            rr = t + h.dt * qv[u] + 2.f * (dy + dz) + (a * (tL - t) + c * (tR - t));
+          }
+        }
+        r[k] = rr;
+        sy[k] = dy;
+        ca[k] = a;
+        cc[k] = c;
+        av[u] = a;
+        cv[u] = c;
+      }
+      // the z-1 / z+1 values of these rows have been used: the rows now hold the coefficients
+      *reinterpret_cast<float4 *>(rowA + x4) = make_float4(av[0], av[1], av[2], av[3]);
+      *reinterpret_cast<float4 *>(rowC + x4) = make_float4(cv[0], cv[1], cv[2], cv[3]);
+      tprev = tv[3];
+    }
+  }
+  __syncwarp();
+  // started pivot of row s-1 (W rows of the recurrence before the lane's chunk)
+  float bp = 0.f, cprev = 0.f;
+  if (act && s > 0) {
+    const int i0 = max(0, s - max(h.W, 1));
+    bp = 1.f + rowA[i0] + rowC[i0];
+    for (int i = i0 + 1; i < s; i++) {
+      const float a = rowA[i];
+      bp = fmaf(-a * rowC[i - 1], frcp(bp), 1.f + a + rowC[i]);
+    }
+    cprev = rowC[s - 1];
+  }
+  float fm[K], bm[K], ib[K];
+  lane_pivots<K>(ca, cc, bp, cprev, min(max(nx - s, 0), K), fm, bm, ib);
+  chunk_solve<K, 32>(r, fm, bm, ib, lane);
+  if (act) {
+#pragma unroll
+    for (int k4 = 0; k4 < K / 4; k4++) {
+      const int x4 = s + 4 * k4;
+      *reinterpret_cast<float4 *>(h.A + rowBase + x4) =
+          make_float4(r[4 * k4] - sy[4 * k4], r[4 * k4 + 1] - sy[4 * k4 + 1], r[4 * k4 + 2] - sy[4 * k4 + 2],
+                      r[4 * k4 + 3] - sy[4 * k4 + 3]);
+    }
+  }
+}
+
+template <int K>
+__global__ void __launch_bounds__(256, 2)
+    sx_kernel(const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTr,
+              const __grid_constant__ CUtensorMap mQr, const __grid_constant__ CUtensorMap mMh,
+              const __grid_constant__ CUtensorMap mCr, const StreamDev h) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = align1024(smem_raw);
+  const XLayout lay = x_layout(h.px, h.Q != nullptr);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * lay.stage);
+  const int yTiles = (h.ny + kXL - 1) / kXL;
+  const int nTiles = yTiles * h.nz;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && h.nS > 0) record_sensors_p(h, *h.stepCounter);
+  auto issue = [&](int tile, int st) {
+    unsigned char *b = smem + st * lay.stage;
+    const int y0 = (tile % yTiles) * kXL, z = tile / yTiles;
+    mbar_expect_tx(&bar[st], lay.tx);
+    tma_load_3d(b, &mTh, 0, y0 - 1, z, &bar[st]);
+    tma_load_3d(b + lay.offTm, &mTr, 0, y0, z - 1, &bar[st]);
+    tma_load_3d(b + lay.offTp, &mTr, 0, y0, z + 1, &bar[st]);
+    if (h.Q) tma_load_3d(b + lay.offQ, &mQr, 0, y0, z, &bar[st]);
+    tma_load_3d(b + lay.offM, &mMh, 0, y0 - 1, z, &bar[st]);
+    tma_load_3d(b + lay.offC, &mCr, 0, y0, z, &bar[st]);
+  };
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; k++) {
+      const int t = blockIdx.x + k * gridDim.x;
+      if (t < nTiles) issue(t, k);
+    }
+  }
+  const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
+  int it = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
+    const int st = it & 1;
+    if (!mbar_wait_bounded(&bar[st], (it >> 1) & 1)) {
+      if (lane == 0) atomicExch(h.err, 1);
+      return;
+    }
+    unsigned char *b = smem + st * lay.stage;
+    const int y0 = (tile % yTiles) * kXL, z = tile / yTiles;
+    if (y0 + l < h.ny) x_line<K>(h, b, lay, l, y0 + l, z, lane);
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nt = tile + 2 * gridDim.x;
+      if (nt < nTiles) issue(nt, st);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Y and Z passes
+// ---------------------------------------------------------------------------------------------
+
+template <int K, int G, bool ZP>
+__global__ void __launch_bounds__(16 * G, 2)
+    syz_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mM,
+               const __grid_constant__ CUtensorMap mT, const StreamDev h) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = align1024(smem_raw);
+  __shared__ unsigned int mloc[256];
+  const int nx = h.nx;
+  const int n = ZP ? h.nz : h.ny;
+  const int d = ZP ? 2 : 1;
+  const YZLayout lay = yz_layout(n, ZP);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * lay.stage);
+  const int xTiles = (nx + kTW - 1) / kTW;
+  const int nOther = ZP ? h.ny : h.nz;
+  const int nTiles = xTiles * nOther;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (ZP)
+    for (int k = threadIdx.x; k < h.nM; k += blockDim.x) mloc[k] = 0u;
+  __syncthreads();
+  auto issue = [&](int tile, int st) {
+    unsigned char *b = smem + st * lay.stage;
+    const int x0 = (tile % xTiles) * kTW, o = tile / xTiles;
+    mbar_expect_tx(&bar[st], lay.tx);
+    for (int k = 0; k < lay.nb; k++) {
+      const int r0 = k * lay.BN;
+      if (ZP) {
+        tma_load_3d(b + r0 * 64, &mA, x0 / 2, o, r0, &bar[st]);
+        tma_load_3d(b + lay.offM + r0 * 16, &mM, x0 / 4, o, r0, &bar[st]);
+        tma_load_3d(b + lay.offT + r0 * 64, &mT, x0 / 2, o, r0, &bar[st]);
+      } else {
+        tma_load_3d(b + r0 * 64, &mA, x0 / 2, r0, o, &bar[st]);
+        tma_load_3d(b + lay.offM + r0 * 16, &mM, x0 / 4, r0, o, &bar[st]);
+      }
+    }
+  };
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; k++) {
+      const int t = blockIdx.x + k * gridDim.x;
+      if (t < nTiles) issue(t, k);
+    }
+  }
+  const int j = threadIdx.x / G, g = threadIdx.x % G;
+  const int kk = (n + G - 1) / G;
+  const int s = g * kk, e = min(s + kk, n);
+  const int dn = d * h.nM * h.nM;
+  int curM = -1;
+  unsigned int curMax = 0u;
+  int it = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
+    const int st = it & 1;
+    if (!mbar_wait_bounded(&bar[st], (it >> 1) & 1)) {
+      if (threadIdx.x == 0) atomicExch(h.err, 2);
+      break;
+    }
+    unsigned char *b = smem + st * lay.stage;
+    float *At = reinterpret_cast<float *>(b);
+    const uint8_t *Mt = b + lay.offM;
+    const float *Tt = reinterpret_cast<const float *>(b + lay.offT);
+    const int x0 = (tile % xTiles) * kTW, o = tile / xTiles;
+    const int x = x0 + j;
+    const bool colValid = x < nx;
+    // the whole line is heat-sinked when it lies on a boundary face of the other two axes
+    const bool lineSink = h.hs && (x == 0 || x == nx - 1 || o == 0 || o == nOther - 1);
+    auto at = [&](const float *tile_, int i) { return *reinterpret_cast<const float *>(reinterpret_cast<const unsigned char *>(tile_) + swz(i, j)); };
+    auto med = [&](int i) { return (int)Mt[i * kTW + j]; };
+    auto coef = [&](int i, int mi, int mprev, int mnext, float &a, float &c) {
+      a = c = 0.f;
+      if (lineSink || (h.hs && (i == 0 || i == n - 1))) return;
+      const float hm = __ldg(h.H + dn + mi * h.nM + mi);
+      if (i > 0) a = mprev == mi ? hm : __ldg(h.H + dn + mprev * h.nM + mi);
+      if (i < n - 1) c = mnext == mi ? hm : __ldg(h.H + dn + mnext * h.nM + mi);
+    };
+    float r[K], ca[K], cc[K];
+    {
+      int mprev = s > 0 ? med(s - 1) : 0, mcur = med(min(s, n - 1));
+      float tprev = 0.f, tcur = 0.f;
+      if (ZP) {
+        tprev = s > 0 ? at(Tt, s - 1) : 0.f;
+        tcur = at(Tt, min(s, n - 1));
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const int i = s + k;
+        r[k] = ca[k] = cc[k] = 0.f;
+        if (k < kk && i < e) {
+          const int mnext = i + 1 < n ? med(i + 1) : 0;
+          float a, c;
+          coef(i, mcur, mprev, mnext, a, c);
+          float rhs = at(At, i);
+          if (ZP) {
+            const float tnext = i + 1 < n ? at(Tt, i + 1) : 0.f;
+            rhs -= a * (tprev - tcur) + c * (tnext - tcur);  // A2 - S_z (3a)
+            tprev = tcur;
+            tcur = tnext;
+          }
+          r[k] = colValid ? rhs : 0.f;
+          ca[k] = a;
+          cc[k] = c;
+          mprev = mcur;
+          mcur = mnext;
+        }
+      }
+    }
+    float bp = 0.f, cprev = 0.f;
+    if (s > 0 && s < n) {
+      const int i0 = max(0, s - max(h.W, 1));
+      int mp = i0 > 0 ? med(i0 - 1) : 0, mc = med(i0);
+      float a, c;
+      int mn = med(i0 + 1);
+      coef(i0, mc, mp, mn, a, c);
+      bp = 1.f + a + c;
+      for (int i = i0 + 1; i < s; i++) {
+        mp = mc;
+        mc = mn;
+        mn = i + 1 < n ? med(i + 1) : 0;
+        const float cpre = c;
+        coef(i, mc, mp, mn, a, c);
+        bp = fmaf(-a * cpre, frcp(bp), 1.f + a + c);
+      }
+      cprev = c;
+    }
+    float fm[K], bm[K], ib[K];
+    lane_pivots<K>(ca, cc, bp, cprev, max(e - s, 0), fm, bm, ib);
+    chunk_solve<K, G>(r, fm, bm, ib, g);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int i = s + k;
+      if (k < kk && i < e) *reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(At) + swz(i, j)) = colValid ? r[k] : 0.f;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < lay.nb; k++) {
+        const int r0 = k * lay.BN;
+        if (ZP) tma_store_3d(&mT, x0 / 2, o, r0, b + r0 * 64);
+        else tma_store_3d(&mA, x0 / 2, r0, o, b + r0 * 64);
+      }
+      tma_store_commit();
+    }
+    if (ZP) {
+      // damage with the mid-step temperature (finiteElementHeatPropagator.c:600-602) and the
+      // running per-medium maxima, over the tile in x-contiguous order
+      for (int q = threadIdx.x; q < kTW * n; q += blockDim.x) {
+        const int i = q >> 4, jj = q & 15, xx = x0 + jj;
+        if (xx >= nx) continue;
+        const int off = i * 64 + ((((jj >> 2) ^ (i >> 1)) & 3) << 4) + ((jj & 3) << 2);
+        const float tnew = *reinterpret_cast<const float *>(b + off);
+        const int m = Mt[i * kTW + jj];
+        const float2 dg = h.dmg[m];
+        if (h.dOmega && dg.y > 0.f) {
+          // log A - E / (R (T0 + d)) = x0 + (E/R) d / (T0 (T0 + d)), x0 formed in FP64 per call
+          const float told = *reinterpret_cast<const float *>(b + lay.offT + off);
+          const float dm = 0.5f * (tnew + told);
+          h.dOmega[xx + (long long)o * h.px + (long long)i * h.sxy] += h.dt * expf(dg.x + dg.y * dm / (h.T0 * (h.T0 + dm)));
+        }
+        const unsigned int enc = enc_max((float)((double)tnew + h.base));
+        if (m != curM) {
+          if (curM >= 0) atomicMax(&mloc[curM], curMax);
+          curM = m;
+          curMax = enc;
+        } else if (enc > curMax) {
+          curMax = enc;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nt = tile + 2 * gridDim.x;
+      tma_store_wait_read();
+      if (nt < nTiles) {
+        fence_proxy_async();
+        issue(nt, st);
+      }
+    }
+  }
+  if (threadIdx.x == 0) tma_store_wait_all();
+  if (ZP) {
+    if (curM >= 0) atomicMax(&mloc[curM], curMax);
+    __syncthreads();
+    for (int k = threadIdx.x; k < h.nM; k += blockDim.x)
+      if (mloc[k]) atomicMax(&h.maxEnc[k], mloc[k]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(h.stepCounter, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Layout conversions and per-call set-up kernels
+// ---------------------------------------------------------------------------------------------
+
+struct Pitch {
+  int nx, ny, nz, px;
+  __device__ __forceinline__ long long p(long long v) const {
+    const long long nxy = (long long)nx * ny;
+    const long long iz = v / nxy, r = v - iz * nxy, iy = r / nx, ix = r - iy * nx;
+    return ix + (iy + iz * ny) * px;
+  }
+};
+
+__global__ void to_pitched_dev_kernel(const float *dense, float *out, double base, Pitch P, long long L) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
+    out[P.p(v)] = (float)((double)dense[v] - base);
+}
+
+__global__ void from_pitched_dev_kernel(const float *pitched, float *dense, double base, Pitch P, long long L) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
+    dense[v] = (float)((double)pitched[P.p(v)] + base);
+}
+
+__global__ void to_pitched_f32_kernel(const float *dense, float *out, Pitch P, long long L) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
+    out[P.p(v)] = dense[v];
+}
+
+__global__ void to_pitched_u8_kernel(const uint8_t *dense, uint8_t *out, Pitch P, long long L) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
+    out[P.p(v)] = dense[v];
+}
+
+// Neighbourhood code (once per call): bit 2d (2d+1) set when the lower (upper) neighbour along d
+// is missing or of another medium; kCodeSink marks heat-sinked voxels (held fixed).
+__global__ void code_kernel(const uint8_t *M, uint8_t *code, Pitch P, int hs, long long L) {
+  const long long px = P.px, sxy = px * P.ny;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
+    const long long nxy = (long long)P.nx * P.ny;
+    const int iz = (int)(v / nxy);
+    const long long r = v - iz * nxy;
+    const int iy = (int)(r / P.nx), ix = (int)(r - (long long)iy * P.nx);
+    const long long p = ix + iy * px + iz * sxy;
+    const int m = M[p];
+    int c = 0;
+    if (hs && (ix == 0 || ix == P.nx - 1 || iy == 0 || iy == P.ny - 1 || iz == 0 || iz == P.nz - 1)) c = kCodeSink;
+    if (ix == 0 || M[p - 1] != m) c |= 1;
+    if (ix == P.nx - 1 || M[p + 1] != m) c |= 2;
+    if (iy == 0 || M[p - px] != m) c |= 4;
+    if (iy == P.ny - 1 || M[p + px] != m) c |= 8;
+    if (iz == 0 || M[p - sxy] != m) c |= 16;
+    if (iz == P.nz - 1 || M[p + sxy] != m) c |= 32;
+    code[p] = (uint8_t)c;
+  }
+}
+
+__global__ void merge_omega_p_kernel(float *Omega, const float *dOmega, Pitch P, long long L) {
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
+    Omega[v] = (float)((double)Omega[v] + (double)dOmega[P.p(v)]);
+}
+
+__global__ void final_sensors_p_kernel(StreamDev h) { record_sensors_p(h, *h.stepCounter); }
+
+// H <- hdt * c in place (FP32 products, as the stepper forms its coefficients) and the diagonal
+// table Hd[m] = {H(m, m, 0), H(m, m, 1), H(m, m, 2), 0}. One block writes Hd after its grid-stride
+// pass, from the products it forms itself.
+__global__ void h_table_kernel(float *H, float4 *Hd, float hdt, int nM) {
+  const int n = 3 * nM * nM;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int mi = k % nM, mj = (k / nM) % nM;
+    if (mi != mj) H[k] *= hdt;
+  }
+  if (blockIdx.x == 0) {
+    for (int m = threadIdx.x; m < nM; m += blockDim.x) {
+      float v[3];
+      for (int d = 0; d < 3; d++) {
+        const int k = (d * nM + m) * nM + m;
+        v[d] = hdt * H[k];
+        H[k] = v[d];
+      }
+      Hd[m] = make_float4(v[0], v[1], v[2], 0.f);
+    }
+  }
+}
+
+__global__ void decode_max_p_kernel(const unsigned int *enc, float *out, int nM) {
+  for (int k = threadIdx.x; k < nM; k += blockDim.x) {
+    const unsigned int e = enc[k];
+    if (e == 0u) out[k] = -__int_as_float(0x7f800000);
+    else out[k] = __uint_as_float((e & 0x80000000u) ? (e & 0x7fffffffu) : ~e);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------------
+
+int x_chunk(int nx) { return nx <= 128 ? 4 : nx <= 256 ? 8 : nx <= 384 ? 12 : 16; }
+
+// x pitch: a multiple of 16 that also holds every lane's whole chunk of K voxels
+int pitch_of(int nx) {
+  const int K = x_chunk(nx);
+  const int w = (nx + K - 1) / K * K;
+  return (w + 15) / 16 * 16;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 3D map over a pitched grid. f32 grids are addressed as 8-byte pairs, byte grids as 4-byte quads.
+mcb_status make_map(mcb_ctx *ctx, CUtensorMap *map, void *base, bool f32, const StreamShape &S, int b0, int b1, int b2,
+                    bool swz64) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+  if (!fn) return set_error(ctx, MCB_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const int es = f32 ? 8 : 4;
+  const int per = f32 ? 2 : 4;
+  const int rowBytes = f32 ? 4 * S.px : S.px;
+  cuuint64_t dims[3] = {(cuuint64_t)(S.px / per), (cuuint64_t)S.ny, (cuuint64_t)S.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)rowBytes, (cuuint64_t)rowBytes * S.ny};
+  cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, (cuuint32_t)b2};
+  cuuint32_t estr[3] = {1, 1, 1};
+  (void)es;
+  const CUresult r = fn(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, base, dims, strides,
+                        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(ctx, MCB_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return MCB_OK;
+}
+
+// dynamic shared memory: two stages, the two mbarriers, and 1 KB of alignment slack
+size_t x_smem(int px, bool q) { return 2 * (size_t)x_layout(px, q).stage + 64 + 1024; }
+size_t yz_smem(int n, bool z) { return 2 * (size_t)yz_layout(n, z).stage + 64 + 1024; }
+
+template <int K>
+mcb_status x_attr(mcb_ctx *ctx, size_t bytes) {
+  MCB_CUDA(ctx, cudaFuncSetAttribute(sx_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return MCB_OK;
+}
+
+template <int K, int G, bool Z>
+mcb_status yz_attr(mcb_ctx *ctx, size_t bytes, int *blocksPerSm) {
+  MCB_CUDA(ctx, cudaFuncSetAttribute(syz_kernel<K, G, Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSm, syz_kernel<K, G, Z>, 16 * G, bytes));
+  return MCB_OK;
+}
+
+// Line-length class of the Y/Z passes: K rows per lane, G lanes per line.
+int yz_class(int n) { return n <= 64 ? 0 : n <= 128 ? 1 : n <= 192 ? 2 : n <= 256 ? 3 : n <= 384 ? 4 : 5; }
+
+template <bool Z>
+mcb_status yz_setup(mcb_ctx *ctx, int n, int *bps) {
+  const size_t b = yz_smem(n, Z);
+  switch (yz_class(n)) {
+    case 0: return yz_attr<4, 16, Z>(ctx, b, bps);
+    case 1: return yz_attr<8, 16, Z>(ctx, b, bps);
+    case 2: return yz_attr<12, 16, Z>(ctx, b, bps);
+    case 3: return yz_attr<16, 16, Z>(ctx, b, bps);
+    case 4: return yz_attr<12, 32, Z>(ctx, b, bps);
+    default: return yz_attr<16, 32, Z>(ctx, b, bps);
+  }
+}
+
+template <bool Z>
+void yz_launch(int n, int grid, cudaStream_t st, const CUtensorMap &a, const CUtensorMap &m, const CUtensorMap &t,
+               const StreamDev &h) {
+  const size_t b = yz_smem(n, Z);
+  switch (yz_class(n)) {
+    case 0: syz_kernel<4, 16, Z><<<grid, 256, b, st>>>(a, m, t, h); break;
+    case 1: syz_kernel<8, 16, Z><<<grid, 256, b, st>>>(a, m, t, h); break;
+    case 2: syz_kernel<12, 16, Z><<<grid, 256, b, st>>>(a, m, t, h); break;
+    case 3: syz_kernel<16, 16, Z><<<grid, 256, b, st>>>(a, m, t, h); break;
+    case 4: syz_kernel<12, 32, Z><<<grid, 512, b, st>>>(a, m, t, h); break;
+    default: syz_kernel<16, 32, Z><<<grid, 512, b, st>>>(a, m, t, h); break;
+  }
+}
+
+}  // namespace
+
+bool stream_supported(int nx, int ny, int nz) {
+  if (nx < 2 || ny < 2 || nz < 2 || nx > 512 || ny > 512 || nz > 512) return false;
+  const int px = pitch_of(nx);
+  // 227 KB per block, less the Y/Z kernels' 1 KB of static maxima
+  return x_smem(px, true) <= 226 * 1024 && yz_smem(ny, false) <= 226 * 1024 && yz_smem(nz, true) <= 226 * 1024;
+}
+
+StreamShape stream_shape(int nx, int ny, int nz) {
+  StreamShape S;
+  S.nx = nx;
+  S.ny = ny;
+  S.nz = nz;
+  S.px = pitch_of(nx);
+  S.Lp = (long long)S.px * ny * nz;
+  return S;
+}
+
+// Pivot warm-up length for H = hdt c (see the file comment): rho^W <= 2^-26 with
+// rho = max over medium pairs of a c / (1 + a + c); 1 << 30 (every lane from row 0) when rho >= 1.
+int stream_warmup(const float *c, float hdt, int nM) {
+  double rho = 0.0;
+  for (int d = 0; d < 3; d++)
+    for (int p = 0; p < nM; p++)
+      for (int q = 0; q < nM; q++) {
+        const double a = hdt * c[(size_t)(d * nM + p) * nM + q];  // row q's coupling to its predecessor p
+        const double cc = hdt * c[(size_t)(d * nM + q) * nM + p];  // row p's coupling to its successor q
+        rho = std::max(rho, a * cc / (1.0 + a + cc));
+      }
+  if (!(rho < 1.0)) return 1 << 30;
+  const double target = std::ldexp(1.0, -26);
+  if (rho <= target) return 1;
+  return std::max(1, (int)std::ceil(std::log(target) / std::log(rho)));
+}
+
+mcb_status stream_maps(mcb_ctx *ctx, mcb_heat_state *s) {
+  const StreamShape &S = s->shape;
+  StreamMaps &m = *s->maps;
+  const int xf = S.px / 2, xq = S.px / 4;
+  const YZLayout ly = yz_layout(S.ny, false), lz = yz_layout(S.nz, true);
+  MCB_TRY(make_map(ctx, &m.xTh, s->T, true, S, xf, kXL + 2, 1, false));
+  MCB_TRY(make_map(ctx, &m.xTr, s->T, true, S, xf, kXL, 1, false));
+  // without a source buffer (light never on) the Q map points at T; it is then never loaded
+  MCB_TRY(make_map(ctx, &m.xQr, s->Q ? s->Q : s->T, true, S, xf, kXL, 1, false));
+  MCB_TRY(make_map(ctx, &m.xMh, s->M, false, S, xq, kXL + 2, 1, false));
+  MCB_TRY(make_map(ctx, &m.xCr, s->code, false, S, xq, kXL, 1, false));
+  MCB_TRY(make_map(ctx, &m.yA, s->A, true, S, kTW / 2, ly.BN, 1, true));
+  MCB_TRY(make_map(ctx, &m.yM, s->M, false, S, kTW / 4, ly.BN, 1, false));
+  MCB_TRY(make_map(ctx, &m.zA, s->A, true, S, kTW / 2, 1, lz.BN, true));
+  MCB_TRY(make_map(ctx, &m.zM, s->M, false, S, kTW / 4, 1, lz.BN, false));
+  MCB_TRY(make_map(ctx, &m.zT, s->T, true, S, kTW / 2, 1, lz.BN, true));
+  return MCB_OK;
+}
+
+// Buffers of the streamed state, carved by `take` (256-byte aligned pieces).
+void stream_carve(const std::function<void *(size_t)> &take, mcb_heat_state *s, const mcb_heat_params *p, bool damage,
+                  bool withQ) {
+  const StreamShape S = stream_shape(p->nx, p->ny, p->nz);
+  const long long L = (long long)p->nx * p->ny * p->nz, Lp = S.Lp;
+  const int nM = p->nM, nS = p->nSensors;
+  s->shape = S;
+  s->T = (float *)take(4 * Lp);
+  s->A = (float *)take(4 * Lp);
+  s->Q = withQ ? (float *)take(4 * Lp) : nullptr;
+  s->M = (uint8_t *)take(Lp);
+  s->code = (uint8_t *)take(Lp);
+  s->dOm = damage ? (float *)take(4 * Lp) : nullptr;
+  s->Om = damage ? (float *)take(4 * L) : nullptr;
+  s->stage = (float *)take(4 * (size_t)std::max<long long>(L, nM));
+  s->H = (float *)take(12 * (size_t)nM * nM);
+  s->Hd = (float4 *)take(16 * (size_t)nM);
+  s->dmg = (float2 *)take(8 * (size_t)nM);
+  s->maxEnc = (unsigned int *)take(4 * (size_t)nM);
+  s->step = (int *)take(16);
+  (void)nS;
+}
+
+// Uploads M (pitched), the neighbourhood code, T (pitched deviations from the mean input
+// temperature) and Omega; clears the padding of every pitched grid.
+mcb_status stream_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T, const float *Omega) {
+  cudaStream_t st = ctx->stream;
+  const StreamShape &S = s->shape;
+  const long long L = (long long)S.nx * S.ny * S.nz;
+  const Pitch P{S.nx, S.ny, S.nz, S.px};
+  const int grid = ctx->num_sms * 8;
+  double sum = 0.0;
+  for (long long k = 0; k < L; k++) sum += T[k];
+  s->base = sum / (double)L;
+  MCB_CUDA(ctx, cudaMemsetAsync(s->T, 0, 4 * S.Lp, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->A, 0, 4 * S.Lp, st));
+  if (s->Q) MCB_CUDA(ctx, cudaMemsetAsync(s->Q, 0, 4 * S.Lp, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->M, 0, S.Lp, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->code, 0, S.Lp, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, p->M, L, cudaMemcpyHostToDevice, st));
+  to_pitched_u8_kernel<<<grid, 256, 0, st>>>((const uint8_t *)s->stage, s->M, P, L);
+  code_kernel<<<grid, 256, 0, st>>>(s->M, s->code, P, p->heatBoundaryType != 0, L);
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, T, 4 * L, cudaMemcpyHostToDevice, st));
+  to_pitched_dev_kernel<<<grid, 256, 0, st>>>(s->stage, s->T, s->base, P, L);
+  if (s->Om && Omega) MCB_CUDA(ctx, cudaMemcpyAsync(s->Om, Omega, 4 * L, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaGetLastError());
+  s->codeHs = (int)(p->heatBoundaryType != 0);
+  s->qValid = false;
+  return MCB_OK;
+}
+
+mcb_status stream_upload_q(mcb_ctx *ctx, mcb_heat_state *s, const float *Q) {
+  cudaStream_t st = ctx->stream;
+  const StreamShape &S = s->shape;
+  const long long L = (long long)S.nx * S.ny * S.nz;
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, Q, 4 * L, cudaMemcpyHostToDevice, st));
+  to_pitched_f32_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->stage, s->Q, Pitch{S.nx, S.ny, S.nz, S.px}, L);
+  MCB_CUDA(ctx, cudaGetLastError());
+  s->qValid = true;
+  return MCB_OK;
+}
+
+// Runs p->steps steps on the device-resident streamed state. Sensor and maximum outputs go to
+// host memory; `sens` is the device buffer of the sensor history ([nS x (steps + 1)] doubles).
+mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, double *sensorTemps,
+                       float *maxMediaTemps, bool graphs) {
+  cudaStream_t st = ctx->stream;
+  const StreamShape &S = s->shape;
+  const long long L = (long long)S.nx * S.ny * S.nz, nt = p->steps;
+  const int nM = p->nM, nS = p->nSensors;
+  if (p->lightsOn && !s->qValid) return set_error(ctx, MCB_EINVAL, "dTdt_abs missing while lightsOn");
+  if (s->codeHs != (int)(p->heatBoundaryType != 0)) {
+    code_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->M, s->code, Pitch{S.nx, S.ny, S.nz, S.px}, p->heatBoundaryType != 0, L);
+    s->codeHs = (int)(p->heatBoundaryType != 0);
+  }
+  // per-call tables (no host allocation): H = dt/2 c in FP32, as the stepper multiplies them, and
+  // its diagonal, formed on the device; the damage exponents about the base temperature; and the
+  // pivot warm-up length
+  const float hdt = (float)(p->dt / 2);
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->H, p->dTdtperdeltaT, 12 * (size_t)nM * nM, cudaMemcpyHostToDevice, st));
+  h_table_kernel<<<std::max(1, std::min(1024, (3 * nM * nM + 255) / 256)), 256, 0, st>>>(s->H, s->Hd, hdt, nM);
+  float2 dmg[256];
+  heat_damage_table(p, s->base, dmg);
+  const int W = stream_warmup(p->dTdtperdeltaT, hdt, nM);
+  MCB_CUDA(ctx, cudaMemcpyAsync(s->dmg, dmg, 8 * (size_t)nM, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->maxEnc, 0, 4 * (size_t)nM, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(s->step, 0, 16, st));
+  if (s->dOm) MCB_CUDA(ctx, cudaMemsetAsync(s->dOm, 0, 4 * (size_t)S.Lp, st));
+
+  StreamDev h{};
+  h.nx = S.nx; h.ny = S.ny; h.nz = S.nz; h.nM = nM; h.px = S.px; h.W = std::min(W, std::max({S.nx, S.ny, S.nz}));
+  h.sxy = (long long)S.px * S.ny;
+  h.T = s->T; h.A = s->A; h.M = s->M; h.code = s->code;
+  h.Q = p->lightsOn ? s->Q : nullptr;
+  h.dOmega = s->dOm; h.H = s->H; h.Hd = s->Hd; h.dmg = s->dmg;
+  h.T0 = (float)(s->base + kCelsiusZero); h.dt = (float)p->dt;
+  h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0; h.base = s->base;
+  h.nS = nS; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = sens; h.stepCounter = s->step; h.err = s->step + 1;
+  s->lastW = h.W;
+
+  const int K = x_chunk(S.nx);
+  const size_t xs = x_smem(S.px, h.Q != nullptr);
+  switch (K) {
+    case 4: MCB_TRY(x_attr<4>(ctx, xs)); break;
+    case 8: MCB_TRY(x_attr<8>(ctx, xs)); break;
+    case 12: MCB_TRY(x_attr<12>(ctx, xs)); break;
+    default: MCB_TRY(x_attr<16>(ctx, xs)); break;
+  }
+  int bpsY = 1, bpsZ = 1;
+  MCB_TRY(yz_setup<false>(ctx, S.ny, &bpsY));
+  MCB_TRY(yz_setup<true>(ctx, S.nz, &bpsZ));
+  const int xbps = xs <= 110 * 1024 ? 2 : 1;
+  const long long tilesX = (long long)((S.ny + kXL - 1) / kXL) * S.nz;
+  const long long tilesY = (long long)((S.nx + kTW - 1) / kTW) * S.nz, tilesZ = (long long)((S.nx + kTW - 1) / kTW) * S.ny;
+  const int gX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * xbps);
+  const int gY = (int)std::min<long long>(tilesY, (long long)ctx->num_sms * std::max(1, bpsY));
+  const int gZ = (int)std::min<long long>(tilesZ, (long long)ctx->num_sms * std::max(1, bpsZ));
+  const StreamMaps &mp = *s->maps;
+  auto step = [&](cudaStream_t q) {
+    switch (K) {
+      case 4: sx_kernel<4><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
+      case 8: sx_kernel<8><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
+      case 12: sx_kernel<12><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
+      default: sx_kernel<16><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
+    }
+    yz_launch<false>(S.ny, gY, q, mp.yA, mp.yM, mp.yA, h);
+    yz_launch<true>(S.nz, gZ, q, mp.zA, mp.zM, mp.zT, h);
+  };
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
+  const int chunk = 16;
+  long long done = 0;
+  if (graphs && nt >= chunk) {
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    MCB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; k++) step(st);
+    MCB_CUDA(ctx, cudaStreamEndCapture(st, &graph));
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      MCB_CUDA(ctx, ie);
+    }
+    for (; done + chunk <= nt; done += chunk) {
+      const cudaError_t le = cudaGraphLaunch(exec, st);
+      if (le != cudaSuccess) {
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        MCB_CUDA(ctx, le);
+      }
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+  }
+  for (; done < nt; done++) step(st);
+  if (nS) final_sensors_p_kernel<<<1, 128, 0, st>>>(h);
+  if (s->dOm) merge_omega_p_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->Om, s->dOm, Pitch{S.nx, S.ny, S.nz, S.px}, L);
+  MCB_CUDA(ctx, cudaGetLastError());
+  MCB_CUDA(ctx, cudaEventRecord(ctx->ev1, st));
+  decode_max_p_kernel<<<1, 256, 0, st>>>(s->maxEnc, s->stage, nM);
+  if (maxMediaTemps) MCB_CUDA(ctx, cudaMemcpyAsync(maxMediaTemps, s->stage, 4 * (size_t)nM, cudaMemcpyDeviceToHost, st));
+  if (nS && sensorTemps)
+    MCB_CUDA(ctx, cudaMemcpyAsync(sensorTemps, sens, 8 * (size_t)nS * (nt + 1), cudaMemcpyDeviceToHost, st));
+  int flags[4] = {0, 0, 0, 0};
+  MCB_CUDA(ctx, cudaMemcpyAsync(flags, s->step, 16, cudaMemcpyDeviceToHost, st));
+  MCB_CUDA(ctx, cudaStreamSynchronize(st));
+  if (flags[1]) return set_error(ctx, MCB_ETIMEOUT, "heat stepper: a TMA tile wait timed out (pass %d)", flags[1]);
+  float ms = 0.f;
+  MCB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->lastKernelMs = ms;
+  return MCB_OK;
+}
+
+mcb_status stream_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Omega) {
+  cudaStream_t st = ctx->stream;
+  const StreamShape &S = s->shape;
+  const long long L = (long long)S.nx * S.ny * S.nz;
+  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, s->stage, s->base, Pitch{S.nx, S.ny, S.nz, S.px}, L);
+  MCB_CUDA(ctx, cudaGetLastError());
+  if (T) MCB_CUDA(ctx, cudaMemcpyAsync(T, s->stage, 4 * L, cudaMemcpyDeviceToHost, st));
+  if (Omega && s->Om) MCB_CUDA(ctx, cudaMemcpyAsync(Omega, s->Om, 4 * L, cudaMemcpyDeviceToHost, st));
+  MCB_CUDA(ctx, cudaStreamSynchronize(st));
+  return MCB_OK;
+}
+
+}  // namespace mcb

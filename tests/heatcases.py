@@ -50,3 +50,25 @@ CASES = {
     "hot_damage": hot_damage,
     "no_damage_single_step": no_damage_single_step,
 }
+
+
+def shaped(shape, seed=5, heatSinked=0, lightsOn=True, nt=12, dt_factor=0.9, with_damage=True, size=(1.0, 1.0, 0.6)):
+    """A seeded 4-medium box of any shape (bulk, top layer, deep layer, ellipsoidal target with
+    Arrhenius damage; configs.heat_adjoint_case) with a non-uniform initial temperature, an initial
+    damage field and three temperature sensors: exercises every line-length class of the stepper."""
+    nx, ny, nz = shape
+    c = configs.heat_adjoint_case(shape=shape, size=size, nt=nt, seed=seed, dtFactor=dt_factor, heatBoundaryType=heatSinked)
+    hp = dict(c["hp"])
+    dx, dy, dz = c["d"]
+    x = (np.arange(nx) + 0.5) * dx - size[0] / 2
+    y = (np.arange(ny) + 0.5) * dy - size[1] / 2
+    z = (np.arange(nz) + 0.5) * dz
+    li, w = prep.convert_temp_sensor_pos([[0.0, 0.0, 0.5 * size[2]], [0.21 * size[0], -0.13 * size[1], 0.11 * size[2]],
+                                          [-0.4 * size[0], 0.37 * size[1], 0.83 * size[2]]], x, y, z)
+    hp = mexargs.heat_mex_params(c["M1"], hp["A"], hp["E"], hp["dTdtperdeltaT"], hp["dTdt_abs"], True, heatSinked, li, w,
+                                 lightsOn, nt, hp["dt"])
+    rng = np.random.default_rng(seed + 100)
+    # hot enough (50-60 degC) that the Arrhenius damage of a few steps is well above FP32 rounding
+    T0 = (50.0 + 10.0 * rng.random(shape)).astype(np.float32)
+    O0 = (rng.random(shape) * 1e-3).astype(np.float32) if with_damage else None
+    return dict(T0=np.asfortranarray(T0), Omega0=None if O0 is None else np.asfortranarray(O0), hp=hp, n=tuple(shape))
