@@ -21,6 +21,7 @@ struct StreamMaps {
   CUtensorMap xTh, xTr, xQr, xMh, xCr;  // X pass: T with y halo rows, T rows, Q rows, media with halo, codes
   CUtensorMap yA, yM;                   // Y pass: A and media, 16 columns x whole y lines
   CUtensorMap zA, zM, zT;               // Z pass: A, media and T, 16 columns x whole z lines
+  CUtensorMap cyA, cyM, czA, czM, czT;  // column-layout Y/Z passes: 32 columns x whole lines
 };
 }  // namespace mcb
 

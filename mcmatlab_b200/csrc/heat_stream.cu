@@ -47,12 +47,15 @@ namespace mcb {
 
 namespace {
 
-constexpr int kXL = 8;  // x-lines per X tile, one warp each
+// x-lines per X tile: 8 warps, each solving 32 / G lines (G lanes per line: 16 for x lines up to
+// 128 voxels, 32 beyond)
+__host__ __device__ constexpr int x_lanes(int nx) { return nx <= 128 ? 16 : 32; }
+__host__ __device__ constexpr int x_tile_lines(int nx) { return 8 * (32 / x_lanes(nx)); }
 constexpr int kTW = 16;  // columns per Y/Z tile
 constexpr int kCodeSink = 64;
 
-// Shared-memory layout of one X-tile stage (byte offsets): T rows y0-1..y0+8 of plane z, T rows
-// y0..y0+7 of planes z-1 and z+1, Q rows, medium rows y0-1..y0+8, code rows.
+// Shared-memory layout of one X-tile stage of kXL lines (byte offsets): T rows y0-1..y0+kXL of
+// plane z, T rows y0..y0+kXL-1 of planes z-1 and z+1, Q rows, medium rows y0-1..y0+kXL, code rows.
 struct XLayout {
   int offTm, offTp, offQ, offM, offC, stage;
   uint32_t tx;
@@ -60,7 +63,7 @@ struct XLayout {
 
 __host__ __device__ inline int up128(int b) { return (b + 127) & ~127; }
 
-__host__ __device__ inline XLayout x_layout(int px, bool q) {
+__host__ __device__ inline XLayout x_layout(int px, bool q, int kXL) {
   XLayout L;
   const int rowF = 4 * px;
   L.offTm = up128((kXL + 2) * rowF);
@@ -108,6 +111,7 @@ struct StreamDev {
   float *dOmega;      // or nullptr
   const float *H;     // [3][nM][nM]: H[d*nM*nM + mj*nM + mi] = dt/2 c(mi, mj, d)
   const float4 *Hd;   // [nM] diagonal {H(m,m,0), H(m,m,1), H(m,m,2), 0}
+  const float4 *Hs;   // [nM] 1 / b*(m, d): inverse fixed-point pivot of a line of medium m along d
   const float2 *dmg;  // [nM] Arrhenius exponent about the base temperature
   float T0, dt;
   unsigned int *maxEnc;
@@ -130,8 +134,14 @@ __device__ __forceinline__ unsigned char *align1024(unsigned char *p) {
   return p + (((a + 1023u) & ~1023u) - a);
 }
 
-// Correctly rounded reciprocal: the pivots' rounding enters every step of long runs.
-__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
+// Reciprocal of a pivot (>= 1): the approximate reciprocal refined by one Newton step, within
+// about half an ulp; the pivots' rounding enters every step of long runs, so the bare 1-ulp
+// approximation is not used.
+__device__ __forceinline__ float frcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return fmaf(r, fmaf(-x, r, 1.f), r);
+}
 
 __device__ __forceinline__ float hcoef(const StreamDev &h, int d, int mi, int mj) {
   return __ldg(h.H + (d * h.nM + mj) * h.nM + mi);
@@ -235,8 +245,11 @@ __device__ __forceinline__ void lane_pivots(const float (&a)[K], const float (&c
 // X pass
 // ---------------------------------------------------------------------------------------------
 
-template <int K>
-__device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, const XLayout &lay, int l, int y, int z, int lane) {
+// One x-line (tile row l, grid row y of plane z) solved by the G lanes of an aligned group; an
+// invalid line (past the grid's last row) only takes part in the group's shuffles.
+template <int K, int G>
+__device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, const XLayout &lay, int l, int y, int z, int lane,
+                                       bool valid) {
   const int nx = h.nx, px = h.px;
   const float *Tc = reinterpret_cast<const float *>(b) + (l + 1) * px;
   float *rowA = reinterpret_cast<float *>(b + lay.offTm) + l * px;  // z-1 row, then the line's a_i
@@ -244,8 +257,9 @@ __device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, con
   const float *Qr = h.Q ? reinterpret_cast<const float *>(b + lay.offQ) + l * px : nullptr;
   const uint8_t *Mc = b + lay.offM + (l + 1) * px;
   const uint8_t *Cr = b + lay.offC + l * px;
-  const int s = lane * K;
+  const int s = valid ? lane * K : nx;  // an invalid line holds no rows
   const long long rowBase = (long long)y * px + (long long)z * h.sxy;
+  const bool yLo = y > 0, yHi = y < h.ny - 1, zLo = z > 0, zHi = z < h.nz - 1;
   float r[K], sy[K], ca[K], cc[K];
 #pragma unroll
   for (int k = 0; k < K; k++) r[k] = sy[k] = ca[k] = cc[k] = 0.f;
@@ -279,21 +293,23 @@ __device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, con
         if (x < nx) {
           rr = t;
           if (!(code & kCodeSink)) {
-            if ((code & 63) == 0) {
-              const float4 H = __ldg(h.Hd + m);
-              a = c = H.x;
-              dy = H.y * ((ymv[u] - t) + (ypv[u] - t));
-              dz = H.z * ((zmv[u] - t) + (zpv[u] - t));
-            } else {
-              // a neighbour is missing or of another medium: every face looked up
-              if (x > 0) a = hcoef(h, 0, m, Mc[x - 1]);
-              if (x < nx - 1) c = hcoef(h, 0, m, Mc[x + 1]);
-              if (y > 0) dy += hcoef(h, 1, m, Mc[x - px]) * (ymv[u] - t);
-              if (y < h.ny - 1) dy += hcoef(h, 1, m, Mc[x + px]) * (ypv[u] - t);
+            // faces to missing neighbours carry no coefficient; faces to another medium look the
+            // pair up (rare: interfaces), the others take the medium's diagonal
+            const float4 H = __ldg(h.Hd + m);
+            a = x > 0 ? H.x : 0.f;
+            c = x < nx - 1 ? H.x : 0.f;
+            float aym = yLo ? H.y : 0.f, ayp = yHi ? H.y : 0.f, azm = zLo ? H.z : 0.f, azp = zHi ? H.z : 0.f;
+            if (code & 63) {
               const long long p = rowBase + x;
-              if (z > 0) dz += hcoef(h, 2, m, h.M[p - h.sxy]) * (zmv[u] - t);
-              if (z < h.nz - 1) dz += hcoef(h, 2, m, h.M[p + h.sxy]) * (zpv[u] - t);
+              if (code & 1) a = hcoef(h, 0, m, Mc[x - 1]);
+              if (code & 2) c = hcoef(h, 0, m, Mc[x + 1]);
+              if (code & 4) aym = hcoef(h, 1, m, Mc[x - px]);
+              if (code & 8) ayp = hcoef(h, 1, m, Mc[x + px]);
+              if (code & 16) azm = hcoef(h, 2, m, h.M[p - h.sxy]);
+              if (code & 32) azp = hcoef(h, 2, m, h.M[p + h.sxy]);
             }
+            dy = aym * (ymv[u] - t) + ayp * (ypv[u] - t);
+            dz = azm * (zmv[u] - t) + azp * (zpv[u] - t);
             // rhs of 1a: T + dt (Q + D_y T + D_z T) + dt/2 D_x T, with dt D_y T = 2 S_y
             rr = t + h.dt * qv[u] + 2.f * (dy + dz) + (a * (tL - t) + c * (tR - t));
           }
@@ -312,20 +328,41 @@ __device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, con
     }
   }
   __syncwarp();
-  // started pivot of row s-1 (W rows of the recurrence before the lane's chunk)
-  float bp = 0.f, cprev = 0.f;
-  if (act && s > 0) {
-    const int i0 = max(0, s - max(h.W, 1));
-    bp = 1.f + rowA[i0] + rowC[i0];
-    for (int i = i0 + 1; i < s; i++) {
-      const float a = rowA[i];
-      bp = fmaf(-a * rowC[i - 1], frcp(bp), 1.f + a + rowC[i]);
-    }
-    cprev = rowC[s - 1];
-  }
   float fm[K], bm[K], ib[K];
-  lane_pivots<K>(ca, cc, bp, cprev, min(max(nx - s, 0), K), fm, bm, ib);
-  chunk_solve<K, 32>(r, fm, bm, ib, lane);
+  // homogeneous lanes: rows s - W - 1 .. e of the line all of one medium (code bit 1 clear on rows
+  // s - W - 1 .. e - 1), none heat-sinked, none a line end. Their exact pivots lie within rho^(W+1)
+  // of the medium's fixed point b*, so every row takes a = c = h and 1 / b' = 1 / b*.
+  const int e = min(s + K, nx);
+  bool uni = act && s >= h.W + 1 && e <= nx - 1;
+  for (int i = s - h.W - 1; uni && i <= e; i++) {
+    const int cd = Cr[i];
+    uni = !(cd & kCodeSink) && (i == e || !(cd & 2));
+  }
+  if (uni) {
+    const int m0 = Mc[s];
+    const float ibs = __ldg(&h.Hs[m0].x), f = __ldg(&h.Hd[m0].x) * ibs;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const bool in = k < e - s;
+      fm[k] = in ? f : 1.f;
+      bm[k] = in ? f : 1.f;
+      ib[k] = in ? ibs : 0.f;
+    }
+  } else {
+    // started pivot of row s-1 (W rows of the recurrence before the lane's chunk)
+    float bp = 0.f, cprev = 0.f;
+    if (act && s > 0) {
+      const int i0 = max(0, s - max(h.W, 1));
+      bp = 1.f + rowA[i0] + rowC[i0];
+      for (int i = i0 + 1; i < s; i++) {
+        const float a = rowA[i];
+        bp = fmaf(-a * rowC[i - 1], frcp(bp), 1.f + a + rowC[i]);
+      }
+      cprev = rowC[s - 1];
+    }
+    lane_pivots<K>(ca, cc, bp, cprev, min(max(nx - s, 0), K), fm, bm, ib);
+  }
+  chunk_solve<K, G>(r, fm, bm, ib, lane);
   if (act) {
 #pragma unroll
     for (int k4 = 0; k4 < K / 4; k4++) {
@@ -337,14 +374,15 @@ __device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, con
   }
 }
 
-template <int K>
-__global__ void __launch_bounds__(256, 2)
+template <int K, int G>
+__global__ void __launch_bounds__(256, G == 16 ? 3 : 2)
     sx_kernel(const __grid_constant__ CUtensorMap mTh, const __grid_constant__ CUtensorMap mTr,
               const __grid_constant__ CUtensorMap mQr, const __grid_constant__ CUtensorMap mMh,
               const __grid_constant__ CUtensorMap mCr, const StreamDev h) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = align1024(smem_raw);
-  const XLayout lay = x_layout(h.px, h.Q != nullptr);
+  constexpr int kXL = 8 * (32 / G);
+  const XLayout lay = x_layout(h.px, h.Q != nullptr, kXL);
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * lay.stage);
   const int yTiles = (h.ny + kXL - 1) / kXL;
   const int nTiles = yTiles * h.nz;
@@ -372,17 +410,18 @@ __global__ void __launch_bounds__(256, 2)
       if (t < nTiles) issue(t, k);
     }
   }
-  const int lane = threadIdx.x & 31, l = threadIdx.x >> 5;
+  const int lane = threadIdx.x & (G - 1), l = (threadIdx.x >> 5) * (32 / G) + ((threadIdx.x & 31) / G);
   int it = 0;
   for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
     const int st = it & 1;
     if (!mbar_wait_bounded(&bar[st], (it >> 1) & 1)) {
-      if (lane == 0) atomicExch(h.err, 1);
+      if (threadIdx.x == 0) atomicExch(h.err, 1);
       return;
     }
     unsigned char *b = smem + st * lay.stage;
     const int y0 = (tile % yTiles) * kXL, z = tile / yTiles;
-    if (y0 + l < h.ny) x_line<K>(h, b, lay, l, y0 + l, z, lane);
+    // lines past the grid's last row still take part in the group's shuffles (an empty line)
+    x_line<K, G>(h, b, lay, l, min(y0 + l, h.ny - 1), z, lane, y0 + l < h.ny);
     fence_proxy_async();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -586,6 +625,304 @@ __global__ void __launch_bounds__(16 * G, 2)
 }
 
 // ---------------------------------------------------------------------------------------------
+// Y and Z passes, column layout (lines up to 320 rows)
+// ---------------------------------------------------------------------------------------------
+
+// A block of G warps owns 32 consecutive x columns of whole lines (Y: one z, Z: one y); lane l
+// is column x0 + l in every warp, and warp w holds rows [w*kk, w*kk + kk) of its column in
+// registers (kk = ceil(n / G) <= K). The tiles (A, media, and for Z the T^n rows) are
+// prefetched with TMA into a two-stage shared-memory pipeline of plain 128-byte rows (lane l reads
+// bank l), so the next tile streams in while this one is solved. The chunk maps of both scans are
+// combined across the warps through shared memory (G - 1 fused multiply-adds per carry). The Z
+// pass forms S_z from the T^n rows it holds and adds the damage and the running maxima of its
+// rows before writing T^{n+1}; results leave with coalesced row stores.
+struct ColLayout {
+  int nb, BN, offM, offT, stage, sums;
+  uint32_t tx;
+};
+
+__host__ __device__ inline ColLayout col_layout(int n, bool zpass, int G) {
+  ColLayout L;
+  L.nb = n > 256 ? 2 : 1;
+  L.BN = (((n + L.nb - 1) / L.nb) + 3) & ~3;  // multiple of 4: every box starts 128-byte aligned
+  const int rows = L.nb * L.BN;
+  L.offM = (rows * 128 + 127) & ~127;
+  L.offT = L.offM + ((rows * 32 + 127) & ~127);
+  L.stage = (L.offT + (zpass ? rows * 128 : 0) + 1023) & ~1023;
+  L.sums = 2 * L.stage;
+  L.tx = (uint32_t)(rows * (128 + 32 + (zpass ? 128 : 0)));
+  (void)G;
+  return L;
+}
+
+template <int K, bool ZP, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
+    scol_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mM,
+                const __grid_constant__ CUtensorMap mT, const StreamDev h, int G) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = align1024(smem_raw);
+  __shared__ unsigned int mloc[256];
+  __shared__ float hd[256];   // H(m, m) of this direction
+  __shared__ float hsv[256];  // 1 / b*(m) of this direction
+  const int n = ZP ? h.nz : h.ny;
+  const ColLayout lay = col_layout(n, ZP, G);
+  float2 *sums = reinterpret_cast<float2 *>(smem + lay.sums);  // [2 tiles][2 scans][G][32] chunk maps (A, B)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + lay.sums + 4 * G * 32 * sizeof(float2));
+  const long long st = ZP ? h.sxy : (long long)h.px;
+  const int nOther = ZP ? h.ny : h.nz;
+  const int nx = h.nx, nM = h.nM;
+  const int xTiles = (nx + 31) >> 5;
+  const int nTiles = xTiles * nOther;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int kk = (n + G - 1) / G;
+  const int s = min(w * kk, n), e = min(s + kk, n), cnt = e - s;
+  const float *Hl = h.H + (ZP ? 2 : 1) * nM * nM;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  for (int k = threadIdx.x; k < nM; k += blockDim.x) {
+    hd[k] = Hl[k * nM + k];
+    const float4 f4 = h.Hs[k];
+    hsv[k] = ZP ? f4.z : f4.y;
+    if (ZP) mloc[k] = 0u;
+  }
+  __syncthreads();
+  auto issue = [&](int tile, int stg) {
+    unsigned char *b = smem + stg * lay.stage;
+    const int x0 = (tile % xTiles) << 5, o = tile / xTiles;
+    mbar_expect_tx(&bar[stg], lay.tx);
+    for (int k = 0; k < lay.nb; k++) {
+      const int r0 = k * lay.BN;
+      if (ZP) {
+        tma_load_3d(b + r0 * 128, &mA, x0 / 2, o, r0, &bar[stg]);
+        tma_load_3d(b + lay.offM + r0 * 32, &mM, x0 / 4, o, r0, &bar[stg]);
+        tma_load_3d(b + lay.offT + r0 * 128, &mT, x0 / 2, o, r0, &bar[stg]);
+      } else {
+        tma_load_3d(b + r0 * 128, &mA, x0 / 2, r0, o, &bar[stg]);
+        tma_load_3d(b + lay.offM + r0 * 32, &mM, x0 / 4, r0, o, &bar[stg]);
+      }
+    }
+  };
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; k++) {
+      const int t = blockIdx.x + k * gridDim.x;
+      if (t < nTiles) issue(t, k);
+    }
+  }
+  int curM = -1;
+  float curMax = 0.f;  // running maximum of the deviation in medium curM
+  // warp-collective flush of the lanes in `lanes` (all lanes of the warp call it): lanes flushing
+  // the same medium combine their maxima first, so each medium takes one shared atomic per warp
+  auto flush_max = [&](bool flush) {
+    const unsigned want = __ballot_sync(0xffffffffu, flush && curM >= 0);
+    if (!want) return;
+    if (flush && curM >= 0) {
+      const unsigned peers = __match_any_sync(want, curM);
+      const unsigned enc = __reduce_max_sync(peers, enc_max((float)((double)curMax + h.base)));
+      if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(&mloc[curM], enc);
+    }
+  };
+  int it = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
+    const int stg = it & 1;
+    if (!mbar_wait_bounded(&bar[stg], (it >> 1) & 1)) {
+      if (threadIdx.x == 0) atomicExch(h.err, 3);
+      break;
+    }
+    const unsigned char *b = smem + stg * lay.stage;
+    const float *At = reinterpret_cast<const float *>(b);
+    const uint8_t *Mt = b + lay.offM;
+    const float *Tt = reinterpret_cast<const float *>(b + lay.offT);
+    float2 *sF = sums + (stg * 2 * G) * 32, *sB = sF + G * 32;
+    const int x = ((tile % xTiles) << 5) + l, o = tile / xTiles;
+    const bool colValid = x < nx;
+    const long long base = x + (ZP ? (long long)o * h.px : (long long)o * h.sxy);
+    const bool lineSink = h.hs && (x == 0 || x == nx - 1 || o == 0 || o == nOther - 1);
+    const int nv = colValid ? cnt : 0;  // rows of this lane
+    auto med = [&](int i) { return (int)Mt[i * 32 + l]; };
+    // coupling of row i (medium mi) to a neighbour of medium mj: the diagonal from shared memory,
+    // the pair table only across an interface
+    auto hc = [&](int mi, int mj) { return mi == mj ? hd[mi] : __ldg(Hl + mj * nM + mi); };
+    auto rowSink = [&](int i) { return lineSink || (h.hs && (i == 0 || i == n - 1)); };
+    float r[K], fm[K], bm[K], ib[K];
+    float A = 0.f, B = 1.f;
+    // homogeneous lanes: rows s - W - 1 .. e all of one medium, none heat-sinked, none a line end.
+    // Their exact pivots lie within rho^(W+1) of the medium's fixed point b* (the recurrence
+    // contracts towards it from any start), so every row takes a = c = h, 1 / b' = 1 / b*.
+    bool uni = nv > 0 && !lineSink && s >= h.W + 1 && e <= n - 1;
+    int m0 = uni ? med(s) : 0;
+    for (int i = s - h.W - 1; uni && i <= e; i++) uni = med(i) == m0;
+    if (uni) {
+      const float h0 = hd[m0], ibs = hsv[m0], f = h0 * ibs;
+      float tPrev = ZP ? Tt[(s - 1) * 32 + l] : 0.f, tCur = ZP ? Tt[s * 32 + l] : 0.f;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        fm[k] = bm[k] = 1.f;
+        ib[k] = r[k] = 0.f;
+        if (k < nv) {
+          const int i = s + k;
+          float rhs = At[i * 32 + l];
+          if (ZP) {
+            const float tNext = Tt[(i + 1) * 32 + l];  // i + 1 <= e <= n - 1
+            rhs -= h0 * ((tPrev - tCur) + (tNext - tCur));  // A2 - S_z (3a)
+            tPrev = tCur;
+            tCur = tNext;
+          }
+          fm[k] = bm[k] = f;
+          ib[k] = ibs;
+          r[k] = rhs;
+          A = fmaf(f, A, rhs);
+          B *= f;
+        }
+      }
+    } else {
+    // started pivot of row s-1 from W rows of the recurrence before the chunk
+    float bp = 0.f, cprev = 0.f;
+    if (nv > 0 && s > 0) {
+      const int i0 = max(0, s - max(h.W, 1));
+      int mp = i0 > 0 ? med(i0 - 1) : 0, mc = med(i0), mn = med(i0 + 1);
+      const bool rs0 = rowSink(i0);
+      float a = (rs0 || i0 == 0) ? 0.f : hc(mc, mp), c = rs0 ? 0.f : hc(mc, mn);
+      bp = 1.f + a + c;
+      for (int i = i0 + 1; i < s; i++) {
+        mp = mc;
+        mc = mn;
+        mn = med(i + 1);
+        const float cpre = c;
+        const bool rs = rowSink(i);
+        a = rs ? 0.f : hc(mc, mp);
+        c = rs ? 0.f : hc(mc, mn);
+        bp = fmaf(-a * cpre, frcp(bp), 1.f + a + c);
+      }
+      cprev = c;
+    }
+    // one pass over the lane's rows: coefficients, (Z) A2 - S_z, pivots, forward chunk map
+    float ibp = bp > 0.f ? frcp(bp) : 0.f;
+    int mPrev = (nv > 0 && s > 0) ? med(s - 1) : 0, mCur = nv > 0 ? med(s) : 0;
+    float tPrev = (ZP && nv > 0 && s > 0) ? Tt[(s - 1) * 32 + l] : 0.f, tCur = (ZP && nv > 0) ? Tt[s * 32 + l] : 0.f;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      fm[k] = bm[k] = 1.f;
+      ib[k] = r[k] = 0.f;
+      if (k < nv) {
+        const int i = s + k;
+        const int mNext = i + 1 < n ? med(i + 1) : 0;
+        const bool rs = rowSink(i);
+        const float a = (rs || i == 0) ? 0.f : hc(mCur, mPrev);
+        const float c = (rs || i == n - 1) ? 0.f : hc(mCur, mNext);
+        float rhs = At[i * 32 + l];
+        if (ZP) {
+          const float tNext = i + 1 < n ? Tt[(i + 1) * 32 + l] : 0.f;
+          rhs -= a * (tPrev - tCur) + c * (tNext - tCur);  // A2 - S_z (3a)
+          tPrev = tCur;
+          tCur = tNext;
+        }
+        const float bk = fmaf(-a * cprev, ibp, 1.f + a + c);
+        ib[k] = frcp(bk);
+        fm[k] = a * ibp;
+        bm[k] = c * ib[k];
+        ibp = ib[k];
+        cprev = c;
+        r[k] = rhs;
+        A = fmaf(fm[k], A, rhs);
+        B *= fm[k];
+        mPrev = mCur;
+        mCur = mNext;
+      }
+    }
+    }
+    sF[w * 32 + l] = make_float2(A, B);
+    __syncthreads();
+    float dcar = 0.f;
+    for (int q = 0; q < w; q++) {
+      const float2 m2 = sF[q * 32 + l];
+      dcar = fmaf(m2.y, dcar, m2.x);
+    }
+    A = 0.f;
+    B = 1.f;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      dcar = fmaf(fm[k], dcar, r[k]);
+      r[k] = dcar * ib[k];
+    }
+    // back substitution: chunk map x_in = A + B x_out, combined from the last warp down
+#pragma unroll
+    for (int k = K - 1; k >= 0; k--) {
+      A = fmaf(bm[k], A, r[k]);
+      B *= bm[k];
+    }
+    sB[w * 32 + l] = make_float2(A, B);
+    __syncthreads();
+    float tcar = 0.f;
+    for (int q = G - 1; q > w; q--) {
+      const float2 m2 = sB[q * 32 + l];
+      tcar = fmaf(m2.y, tcar, m2.x);
+    }
+#pragma unroll
+    for (int k = K - 1; k >= 0; k--) {
+      tcar = fmaf(bm[k], tcar, r[k]);
+      r[k] = tcar;
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (k < nv) {
+        const long long v = base + (long long)(s + k) * st;
+        if (ZP) {
+          const float tnew = r[k];
+          const int m = med(s + k);  // the stage still holds this tile (reissued below)
+          if (h.dOmega) {
+            const float2 dg = h.dmg[m];
+            if (dg.y > 0.f) {
+              // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602):
+              // log A - E / (R (T0 + d)) = x0 + (E/R) d / (T0 (T0 + d)), x0 formed in FP64 per call
+              const float dm = 0.5f * (tnew + Tt[(s + k) * 32 + l]);
+              h.dOmega[v] += h.dt * expf(dg.x + dg.y * dm / (h.T0 * (h.T0 + dm)));
+            }
+          }
+          h.T[v] = tnew;
+        } else {
+          h.A[v] = r[k];
+        }
+      }
+      if (ZP) {
+        // running maxima: a lane whose medium changes flushes (warp-collectively, every lane calls)
+        const int mk = k < nv ? med(s + k) : curM;
+        const bool change = mk != curM;
+        flush_max(change);
+        if (k < nv) {
+          if (change) {
+            curM = mk;
+            curMax = r[k];
+          } else {
+            curMax = fmaxf(curMax, r[k]);
+          }
+        }
+      }
+    }
+    // every warp is done with this stage: prefetch the tile after next into it. (The chunk maps
+    // alternate between two buffers by tile parity, so the next tile's map writes cannot meet a
+    // warp still reading this tile's: it passes this barrier first.)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nt = tile + 2 * gridDim.x;
+      if (nt < nTiles) {
+        fence_proxy_async();
+        issue(nt, stg);
+      }
+    }
+  }
+  if (ZP) {
+    flush_max(true);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nM; k += blockDim.x)
+      if (mloc[k]) atomicMax(&h.maxEnc[k], mloc[k]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(h.stepCounter, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Layout conversions and per-call set-up kernels
 // ---------------------------------------------------------------------------------------------
 
@@ -619,7 +956,8 @@ __global__ void to_pitched_u8_kernel(const uint8_t *dense, uint8_t *out, Pitch P
 }
 
 // Neighbourhood code (once per call): bit 2d (2d+1) set when the lower (upper) neighbour along d
-// is missing or of another medium; kCodeSink marks heat-sinked voxels (held fixed).
+// exists and is of another medium (its face coefficient needs the pair table); kCodeSink marks
+// heat-sinked voxels (held fixed). Missing neighbours are masked by position in the passes.
 __global__ void code_kernel(const uint8_t *M, uint8_t *code, Pitch P, int hs, long long L) {
   const long long px = P.px, sxy = px * P.ny;
   for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x) {
@@ -631,12 +969,12 @@ __global__ void code_kernel(const uint8_t *M, uint8_t *code, Pitch P, int hs, lo
     const int m = M[p];
     int c = 0;
     if (hs && (ix == 0 || ix == P.nx - 1 || iy == 0 || iy == P.ny - 1 || iz == 0 || iz == P.nz - 1)) c = kCodeSink;
-    if (ix == 0 || M[p - 1] != m) c |= 1;
-    if (ix == P.nx - 1 || M[p + 1] != m) c |= 2;
-    if (iy == 0 || M[p - px] != m) c |= 4;
-    if (iy == P.ny - 1 || M[p + px] != m) c |= 8;
-    if (iz == 0 || M[p - sxy] != m) c |= 16;
-    if (iz == P.nz - 1 || M[p + sxy] != m) c |= 32;
+    if (ix > 0 && M[p - 1] != m) c |= 1;
+    if (ix < P.nx - 1 && M[p + 1] != m) c |= 2;
+    if (iy > 0 && M[p - px] != m) c |= 4;
+    if (iy < P.ny - 1 && M[p + px] != m) c |= 8;
+    if (iz > 0 && M[p - sxy] != m) c |= 16;
+    if (iz < P.nz - 1 && M[p + sxy] != m) c |= 32;
     code[p] = (uint8_t)c;
   }
 }
@@ -648,9 +986,11 @@ __global__ void merge_omega_p_kernel(float *Omega, const float *dOmega, Pitch P,
 
 __global__ void final_sensors_p_kernel(StreamDev h) { record_sensors_p(h, *h.stepCounter); }
 
-// H <- hdt * c in place (FP32 products, as the stepper forms its coefficients) and the diagonal
-// table Hd[m] = {H(m, m, 0), H(m, m, 1), H(m, m, 2), 0}. One block writes Hd after its grid-stride
-// pass, from the products it forms itself.
+// H <- hdt * c in place (FP32 products, as the stepper forms its coefficients), the diagonal table
+// Hd[m] = {H(m, m, 0), H(m, m, 1), H(m, m, 2), 0}, and Hs[m] = 1 / b* per direction, b* the fixed
+// point of the pivot recurrence b -> 1 + 2h - h^2 / b of a line of one medium (h = H(m, m, d)):
+// b* = (1 + 2h + sqrt(1 + 4h)) / 2, in FP64. One block writes Hd and Hs after its grid-stride pass,
+// from the products it forms itself.
 __global__ void h_table_kernel(float *H, float4 *Hd, float hdt, int nM) {
   const int n = 3 * nM * nM;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -659,13 +999,16 @@ __global__ void h_table_kernel(float *H, float4 *Hd, float hdt, int nM) {
   }
   if (blockIdx.x == 0) {
     for (int m = threadIdx.x; m < nM; m += blockDim.x) {
-      float v[3];
+      float v[3], ibs[3];
       for (int d = 0; d < 3; d++) {
         const int k = (d * nM + m) * nM + m;
         v[d] = hdt * H[k];
         H[k] = v[d];
+        const double hh = v[d];
+        ibs[d] = (float)(2.0 / (1.0 + 2.0 * hh + sqrt(1.0 + 4.0 * hh)));
       }
       Hd[m] = make_float4(v[0], v[1], v[2], 0.f);
+      Hd[nM + m] = make_float4(ibs[0], ibs[1], ibs[2], 0.f);
     }
   }
 }
@@ -682,7 +1025,8 @@ __global__ void decode_max_p_kernel(const unsigned int *enc, float *out, int nM)
 // Host side
 // ---------------------------------------------------------------------------------------------
 
-int x_chunk(int nx) { return nx <= 128 ? 4 : nx <= 256 ? 8 : nx <= 384 ? 12 : 16; }
+// voxels per lane of an x-line: 16 lanes x 8 up to 128 voxels, then 32 lanes x 8, 12 or 16
+int x_chunk(int nx) { return nx <= 256 ? 8 : nx <= 384 ? 12 : 16; }
 
 // x pitch: a multiple of 16 that also holds every lane's whole chunk of K voxels
 int pitch_of(int nx) {
@@ -725,12 +1069,12 @@ mcb_status make_map(mcb_ctx *ctx, CUtensorMap *map, void *base, bool f32, const 
 }
 
 // dynamic shared memory: two stages, the two mbarriers, and 1 KB of alignment slack
-size_t x_smem(int px, bool q) { return 2 * (size_t)x_layout(px, q).stage + 64 + 1024; }
+size_t x_smem(int px, bool q, int nx) { return 2 * (size_t)x_layout(px, q, x_tile_lines(nx)).stage + 64 + 1024; }
 size_t yz_smem(int n, bool z) { return 2 * (size_t)yz_layout(n, z).stage + 64 + 1024; }
 
-template <int K>
+template <int K, int G>
 mcb_status x_attr(mcb_ctx *ctx, size_t bytes) {
-  MCB_CUDA(ctx, cudaFuncSetAttribute(sx_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  MCB_CUDA(ctx, cudaFuncSetAttribute(sx_kernel<K, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   return MCB_OK;
 }
 
@@ -743,6 +1087,45 @@ mcb_status yz_attr(mcb_ctx *ctx, size_t bytes, int *blocksPerSm) {
 
 // Line-length class of the Y/Z passes: K rows per lane, G lanes per line.
 int yz_class(int n) { return n <= 64 ? 0 : n <= 128 ? 1 : n <= 192 ? 2 : n <= 256 ? 3 : n <= 384 ? 4 : 5; }
+
+// Column-layout Y/Z pass (lines up to 320 rows): 8 rows per lane for lines up to 256 rows, 16
+// beyond; G = ceil(n / rows) warps.
+constexpr int kColMaxN = 320;
+int col_rows(int n) { return n <= 256 ? 8 : 16; }
+int col_warps(int n) { return (n + col_rows(n) - 1) / col_rows(n); }
+size_t col_smem(int n, bool z) {
+  const int G = col_warps(n);
+  return (size_t)col_layout(n, z, G).sums + 4 * G * 32 * sizeof(float2) + 64 + 1024;
+}
+
+template <int K, bool Z, int MAXT>
+mcb_status col_attr(mcb_ctx *ctx, int n, int *bps) {
+  const size_t sm = col_smem(n, Z);
+  MCB_CUDA(ctx, cudaFuncSetAttribute(scol_kernel<K, Z, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, scol_kernel<K, Z, MAXT>, 32 * col_warps(n), sm));
+  return MCB_OK;
+}
+
+// block-size classes: up to 256 threads (3 blocks per SM), 512 (2), 1024 (1; 16-row lanes: 640)
+template <bool Z>
+mcb_status col_occupancy(mcb_ctx *ctx, int n, int *bps) {
+  const int G = col_warps(n);
+  if (col_rows(n) == 16) return col_attr<16, Z, 640>(ctx, n, bps);
+  if (G <= 8) return col_attr<8, Z, 256>(ctx, n, bps);
+  if (G <= 16) return col_attr<8, Z, 512>(ctx, n, bps);
+  return col_attr<8, Z, 1024>(ctx, n, bps);
+}
+
+template <bool Z>
+void col_launch(int n, int grid, cudaStream_t st, const CUtensorMap &a, const CUtensorMap &m, const CUtensorMap &t,
+                const StreamDev &h) {
+  const int G = col_warps(n);
+  const size_t sm = col_smem(n, Z);
+  if (col_rows(n) == 16) scol_kernel<16, Z, 640><<<grid, 32 * G, sm, st>>>(a, m, t, h, G);
+  else if (G <= 8) scol_kernel<8, Z, 256><<<grid, 32 * G, sm, st>>>(a, m, t, h, G);
+  else if (G <= 16) scol_kernel<8, Z, 512><<<grid, 32 * G, sm, st>>>(a, m, t, h, G);
+  else scol_kernel<8, Z, 1024><<<grid, 32 * G, sm, st>>>(a, m, t, h, G);
+}
 
 template <bool Z>
 mcb_status yz_setup(mcb_ctx *ctx, int n, int *bps) {
@@ -777,7 +1160,8 @@ bool stream_supported(int nx, int ny, int nz) {
   if (nx < 2 || ny < 2 || nz < 2 || nx > 512 || ny > 512 || nz > 512) return false;
   const int px = pitch_of(nx);
   // 227 KB per block, less the Y/Z kernels' 1 KB of static maxima
-  return x_smem(px, true) <= 226 * 1024 && yz_smem(ny, false) <= 226 * 1024 && yz_smem(nz, true) <= 226 * 1024;
+  return x_smem(px, true, nx) <= 226 * 1024 && yz_smem(ny, false) <= 226 * 1024 && yz_smem(nz, true) <= 226 * 1024 &&
+         (ny > kColMaxN || col_smem(ny, false) <= 226 * 1024) && (nz > kColMaxN || col_smem(nz, true) <= 226 * 1024);
 }
 
 StreamShape stream_shape(int nx, int ny, int nz) {
@@ -812,6 +1196,7 @@ mcb_status stream_maps(mcb_ctx *ctx, mcb_heat_state *s) {
   StreamMaps &m = *s->maps;
   const int xf = S.px / 2, xq = S.px / 4;
   const YZLayout ly = yz_layout(S.ny, false), lz = yz_layout(S.nz, true);
+  const int kXL = x_tile_lines(S.nx);
   MCB_TRY(make_map(ctx, &m.xTh, s->T, true, S, xf, kXL + 2, 1, false));
   MCB_TRY(make_map(ctx, &m.xTr, s->T, true, S, xf, kXL, 1, false));
   // without a source buffer (light never on) the Q map points at T; it is then never loaded
@@ -823,6 +1208,18 @@ mcb_status stream_maps(mcb_ctx *ctx, mcb_heat_state *s) {
   MCB_TRY(make_map(ctx, &m.zA, s->A, true, S, kTW / 2, 1, lz.BN, true));
   MCB_TRY(make_map(ctx, &m.zM, s->M, false, S, kTW / 4, 1, lz.BN, false));
   MCB_TRY(make_map(ctx, &m.zT, s->T, true, S, kTW / 2, 1, lz.BN, true));
+  // column-layout Y/Z tiles: 32 columns (16 pairs, 8 quads) of whole lines, plain rows
+  if (S.ny <= kColMaxN) {
+    const ColLayout cy = col_layout(S.ny, false, col_warps(S.ny));
+    MCB_TRY(make_map(ctx, &m.cyA, s->A, true, S, 16, cy.BN, 1, false));
+    MCB_TRY(make_map(ctx, &m.cyM, s->M, false, S, 8, cy.BN, 1, false));
+  }
+  if (S.nz <= kColMaxN) {
+    const ColLayout cz = col_layout(S.nz, true, col_warps(S.nz));
+    MCB_TRY(make_map(ctx, &m.czA, s->A, true, S, 16, 1, cz.BN, false));
+    MCB_TRY(make_map(ctx, &m.czM, s->M, false, S, 8, 1, cz.BN, false));
+    MCB_TRY(make_map(ctx, &m.czT, s->T, true, S, 16, 1, cz.BN, false));
+  }
   return MCB_OK;
 }
 
@@ -842,7 +1239,7 @@ void stream_carve(const std::function<void *(size_t)> &take, mcb_heat_state *s, 
   s->Om = damage ? (float *)take(4 * L) : nullptr;
   s->stage = (float *)take(4 * (size_t)std::max<long long>(L, nM));
   s->H = (float *)take(12 * (size_t)nM * nM);
-  s->Hd = (float4 *)take(16 * (size_t)nM);
+  s->Hd = (float4 *)take(32 * (size_t)nM);  // Hd, then the fixed-point table Hs
   s->dmg = (float2 *)take(8 * (size_t)nM);
   s->maxEnc = (unsigned int *)take(4 * (size_t)nM);
   s->step = (int *)take(16);
@@ -920,39 +1317,41 @@ mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   h.sxy = (long long)S.px * S.ny;
   h.T = s->T; h.A = s->A; h.M = s->M; h.code = s->code;
   h.Q = p->lightsOn ? s->Q : nullptr;
-  h.dOmega = s->dOm; h.H = s->H; h.Hd = s->Hd; h.dmg = s->dmg;
+  h.dOmega = s->dOm; h.H = s->H; h.Hd = s->Hd; h.Hs = s->Hd + nM; h.dmg = s->dmg;
   h.T0 = (float)(s->base + kCelsiusZero); h.dt = (float)p->dt;
   h.maxEnc = s->maxEnc; h.hs = p->heatBoundaryType != 0; h.base = s->base;
   h.nS = nS; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = sens; h.stepCounter = s->step; h.err = s->step + 1;
   s->lastW = h.W;
 
-  const int K = x_chunk(S.nx);
-  const size_t xs = x_smem(S.px, h.Q != nullptr);
-  switch (K) {
-    case 4: MCB_TRY(x_attr<4>(ctx, xs)); break;
-    case 8: MCB_TRY(x_attr<8>(ctx, xs)); break;
-    case 12: MCB_TRY(x_attr<12>(ctx, xs)); break;
-    default: MCB_TRY(x_attr<16>(ctx, xs)); break;
-  }
+  const int K = x_chunk(S.nx), XG = x_lanes(S.nx), XL = x_tile_lines(S.nx);
+  const size_t xs = x_smem(S.px, h.Q != nullptr, S.nx);
+  if (XG == 16) MCB_TRY((x_attr<8, 16>(ctx, xs)));
+  else if (K == 8) MCB_TRY((x_attr<8, 32>(ctx, xs)));
+  else if (K == 12) MCB_TRY((x_attr<12, 32>(ctx, xs)));
+  else MCB_TRY((x_attr<16, 32>(ctx, xs)));
   int bpsY = 1, bpsZ = 1;
-  MCB_TRY(yz_setup<false>(ctx, S.ny, &bpsY));
-  MCB_TRY(yz_setup<true>(ctx, S.nz, &bpsZ));
-  const int xbps = xs <= 110 * 1024 ? 2 : 1;
-  const long long tilesX = (long long)((S.ny + kXL - 1) / kXL) * S.nz;
-  const long long tilesY = (long long)((S.nx + kTW - 1) / kTW) * S.nz, tilesZ = (long long)((S.nx + kTW - 1) / kTW) * S.ny;
+  const bool colY = S.ny <= kColMaxN, colZ = S.nz <= kColMaxN;
+  if (colY) MCB_TRY(col_occupancy<false>(ctx, S.ny, &bpsY));
+  else MCB_TRY(yz_setup<false>(ctx, S.ny, &bpsY));
+  if (colZ) MCB_TRY(col_occupancy<true>(ctx, S.nz, &bpsZ));
+  else MCB_TRY(yz_setup<true>(ctx, S.nz, &bpsZ));
+  const int xbps = std::max(1, std::min(XG == 16 ? 3 : 2, (int)((227u * 1024u) / (unsigned)(xs + 1024))));
+  const long long tilesX = (long long)((S.ny + XL - 1) / XL) * S.nz;
+  const long long tilesY = (long long)((S.nx + (colY ? 31 : kTW - 1)) / (colY ? 32 : kTW)) * S.nz;
+  const long long tilesZ = (long long)((S.nx + (colZ ? 31 : kTW - 1)) / (colZ ? 32 : kTW)) * S.ny;
   const int gX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * xbps);
   const int gY = (int)std::min<long long>(tilesY, (long long)ctx->num_sms * std::max(1, bpsY));
   const int gZ = (int)std::min<long long>(tilesZ, (long long)ctx->num_sms * std::max(1, bpsZ));
   const StreamMaps &mp = *s->maps;
   auto step = [&](cudaStream_t q) {
-    switch (K) {
-      case 4: sx_kernel<4><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
-      case 8: sx_kernel<8><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
-      case 12: sx_kernel<12><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
-      default: sx_kernel<16><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h); break;
-    }
-    yz_launch<false>(S.ny, gY, q, mp.yA, mp.yM, mp.yA, h);
-    yz_launch<true>(S.nz, gZ, q, mp.zA, mp.zM, mp.zT, h);
+    if (XG == 16) sx_kernel<8, 16><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+    else if (K == 8) sx_kernel<8, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+    else if (K == 12) sx_kernel<12, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+    else sx_kernel<16, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+    if (colY) col_launch<false>(S.ny, gY, q, mp.cyA, mp.cyM, mp.cyA, h);
+    else yz_launch<false>(S.ny, gY, q, mp.yA, mp.yM, mp.yA, h);
+    if (colZ) col_launch<true>(S.nz, gZ, q, mp.czA, mp.czM, mp.czT, h);
+    else yz_launch<true>(S.nz, gZ, q, mp.zA, mp.zM, mp.zT, h);
   };
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
   const int chunk = 16;

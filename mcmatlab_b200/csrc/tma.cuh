@@ -30,12 +30,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for the phase with the given parity to complete, for at most about `cycles` SM clocks.
-// Returns false on time-out (the caller records an error and leaves).
+// As mbar_try_wait, but a thread whose phase is not complete sleeps until it completes or about
+// `ns` nanoseconds pass, instead of returning at once.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete, for at most about `cycles` SM clocks,
+// sleeping between the checks. Returns false on time-out (the caller records an error and leaves).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long cycles = 4000000000ll) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try_wait(bar, parity))
+  while (!mbar_try_wait_sleep(bar, parity, 100000u))
     if (clock64() - t0 > cycles) return false;
   return true;
 }
