@@ -187,6 +187,16 @@ def run_ours(args):
             state.step(hp)
             times.append(native.last_kernel_ms(dev))
     torch.cuda.synchronize()
+    # the light-off phase of the schedule (no source term) on the same resident state
+    hp_off = dict(hp, lightsOn=False)
+    state.step(dict(hp_off, steps=float(min(args.nt, 1000))))
+    off_times = []
+    for _ in range(max(1, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        state.step(hp_off)
+        off_times.append(native.last_kernel_ms(dev))
+    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     dev_ms = float(sum(times))
@@ -213,6 +223,10 @@ def run_ours(args):
     bytes_per_update = 9.0 + 4.0 + 8.0 * frac_dmg
     hbm, src = peaks()
     achieved = bytes_per_update * L * args.nt / (ms_per_step / 1e3) / 1e9
+    # light off: no source read (T read + write, M, and Omega where damage accumulates)
+    off_ms = float(np.mean(off_times))
+    off_bytes = 9.0 + 8.0 * frac_dmg
+    off_achieved = off_bytes * L * args.nt / (off_ms / 1e3) / 1e9
     # one bench step: 3 passes per time step + the maxima decode
     launches = args.steps * (3 * args.nt + 1)
     res = {
@@ -235,11 +249,19 @@ def run_ours(args):
                      "traffic": HEAT_STEP_DRAM_BYTES, "traffic_note": "ncu cold-cache capture, bytes per DG-ADI step",
                      "algorithmic_bytes_per_voxel_update": bytes_per_update,
                      "kernel": "DG-ADI step (pass_x + pass_yz<y> + pass_yz<z>)"},
+        "light_off": {"workload": "same state and dt, light off (the cooling phase of the schedule)",
+                      "value": float(L) * args.nt / (off_ms / 1e3), "unit": "voxel-updates/s", "ms_per_step": off_ms,
+                      "steps": len(off_times),
+                      "roofline": {"bound": "hbm", "achieved": off_achieved, "peak": hbm, "unit": "GB/s",
+                                   "frac": off_achieved / hbm, "peak_source": src,
+                                   "algorithmic_bytes_per_voxel_update": off_bytes}},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "mc": {"metric": "photon packets/s", "workload": "standard-tissue cube 100^3, pencil beam, %d x 1e6 packets" % ws,
                "value": MC_PACKETS * ws / (mc_ms / 1e3), "e2e_value": MC_PACKETS * ws / mc_wall,
                "kernel_ms": mc_ms, "propagation_steps": steps_mc,
+               "free_step_cuts": out.get("freeStepCuts"), "free_step_cut_weight_fraction":
+                   (out.get("freeStepCutWeight", 0.0) / out["nPhotons"]) if out.get("nPhotons") else None,
                "steps_per_s": steps_mc / (mc_ms / 1e3),
                "parallelism": "packets sharded over %d ranks, one NCCL all-reduce of the tallies" % ws if ws > 1 else "1 GPU"},
     }
@@ -260,6 +282,9 @@ def run_ours(args):
         if args.cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
             res["mc"]["cpu_baseline"] = res["cpu_baseline"].pop("mc")
+            c4 = res["cpu_baseline"].pop("heat_c4")
+            if "heat_adjoint" in res:
+                res["heat_adjoint"]["cpu_forward"] = c4
         print(json.dumps(res), flush=True)
     state.close()
     if dist:
@@ -278,11 +303,13 @@ def batched_sweep_measure(dev, n_inst, scale):
     native.mc_run(dict(ins[0], nPhotonsRequested=1e4), device=dev)
     native.mc_run_batch([dict(x, nPhotonsRequested=1e3) for x in ins[:4]], device=dev)
     plain_ms = plain_wall = 0.0
+    per_inst = []
     for x in ins:
         t0 = time.perf_counter()
         o = native.mc_run(x, device=dev)
         plain_wall += time.perf_counter() - t0
         plain_ms += o["kernelMs"]
+        per_inst.append([float(x["nPhotonsRequested"]), int(np.asarray(x["M"]).size), round(float(o["kernelMs"]), 3)])
     t0 = time.perf_counter()
     outs = native.mc_run_batch(ins, device=dev)
     batch_wall = time.perf_counter() - t0
@@ -293,7 +320,10 @@ def batched_sweep_measure(dev, n_inst, scale):
             "batched_packets_per_s": total / (batch_ms / 1e3), "plain_per_instance_packets_per_s": total / (plain_ms / 1e3),
             "ratio_device": plain_ms / batch_ms,
             "batched_e2e_packets_per_s": total / batch_wall, "plain_e2e_packets_per_s": total / plain_wall,
-            "ratio_e2e": plain_wall / batch_wall}
+            "ratio_e2e": plain_wall / batch_wall,
+            "free_step_cuts": float(sum(o["freeStepCuts"] for o in outs)),
+            "free_step_cut_weight_fraction": float(sum(o["freeStepCutWeight"] for o in outs) / sum(o["nPhotons"] for o in outs)),
+            "plain_instances": {"columns": ["packets", "voxels", "plain_kernel_ms"], "rows": per_inst}}
 
 
 def grad_measure(dev, packets, n):
@@ -335,7 +365,7 @@ def adjoint_measure(dev, nt):
             "adjoint_over_forward": (g["forwardMs"] + g["adjointMs"]) / fwd_ms}
 
 
-REF_MC_PACKETS = 1e5
+REF_MC_PACKETS = 1e6
 
 
 def reference_setup(timings=None):
@@ -370,7 +400,18 @@ def cpu_baseline(args, sample_steps):
     t0 = time.perf_counter()
     R.run(T0, O0, hp, nthreads=cores)
     dtw = time.perf_counter() - t0
+    # the heat-adjoint workload's grid (300x300x200), forward steps only
+    case = configs.heat_adjoint_case(nt=args.c4_cpu_steps)
+    nx4, ny4, nz4 = case["n"]
+    R.run(case["T0"], np.float32(np.nan), dict(case["hp"], steps=1.0), nthreads=cores)
+    t0 = time.perf_counter()
+    R.run(case["T0"], np.float32(np.nan), case["hp"], nthreads=cores)
+    dt4 = time.perf_counter() - t0
+    c4 = {"value": nx4 * ny4 * nz4 * args.c4_cpu_steps / dt4, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
+          "sample": "%d DG-ADI steps of the 300x300x200 heat-adjoint workload (forward only, no damage), reference MEX C "
+                    "code (-Ofast -fopenmp) on %d host threads" % (args.c4_cpu_steps, cores)}
     return {"value": N_GRID ** 3 * sample_steps / dtw, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
+            "heat_c4": c4,
             "sample": "%d DG-ADI steps of the same 100^3 workload (light on, damage), reference MEX C code "
                       "(-Ofast -fopenmp) on %d host threads" % (sample_steps, cores),
             "mc": {"value": tm["mc_packets"] / tm["mc_s"], "unit": "photon packets/s", "cores": cores, "kind": "reference",
@@ -429,6 +470,7 @@ def main():
     ap.add_argument("--c3-grid", type=int, default=256)
     ap.add_argument("--no-c4", dest="c4", action="store_false", help="skip the heat-adjoint measurement")
     ap.add_argument("--c4-steps", type=int, default=2000)
+    ap.add_argument("--c4-cpu-steps", type=int, default=10, help="time steps of the CPU reference on the 300x300x200 grid")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

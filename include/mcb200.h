@@ -127,6 +127,10 @@ typedef struct mcb_mc_result {
   /* kernel statistics (not in the reference) */
   uint64_t propagationSteps;   /* propagatePhoton-equivalent sub-steps executed */
   double kernelMs;             /* device time of the transport kernels */
+  /* packets ended by the free-step limit (2e4 propagation sub-steps without a scattering event;
+   * the reference has no such limit) and their remaining weight, summed over wavelengths, in
+   * units of one launched packet's weight */
+  double freeStepCuts, freeStepCutWeight;
 } mcb_mc_result;
 
 /* Replaces MCmatlab.c mexFunction: runs all wavelengths, normalises and writes the outputs. */

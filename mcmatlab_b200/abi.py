@@ -61,6 +61,7 @@ class mcb_mc_result(C.Structure):
         ("nPhotons", C.c_double), ("nPhotonsCollected", C.c_double), ("nThreads", C.c_double),
         ("simulationTime", C.c_double),
         ("propagationSteps", C.c_uint64), ("kernelMs", C.c_double),
+        ("freeStepCuts", C.c_double), ("freeStepCutWeight", C.c_double),
     ]
 
 
@@ -263,6 +264,8 @@ class McResultBuffers:
         out["simulationTime"] = r.simulationTime
         out["propagationSteps"] = int(r.propagationSteps)
         out["kernelMs"] = r.kernelMs
+        out["freeStepCuts"] = r.freeStepCuts
+        out["freeStepCutWeight"] = r.freeStepCutWeight
         n = int(r.examplePathsN)
         out["examplePaths"] = self.paths[:4 * n].reshape(4, n, order="F") if n else np.zeros((4, 0))
         return out

@@ -56,7 +56,8 @@ struct Inst {
   int crit;  // a deposition criterion is set (criteria_met is true otherwise)
   // FP64 tallies
   double *NFR, *image, *FF, *NIxp, *NIxn, *NIyp, *NIyn, *NIzp, *NIzn;
-  unsigned long long *ctr;  // [0] launched, [1] collected, [2] sub-steps, [3] failed launches
+  unsigned long long *ctr;  // [0] launched, [1] collected, [2] unused, [3] failed launches,
+                            // [4] free-step cuts, [5] their weight (a double)
   // RNG stream
   uint32_t key0, key1, ctr2hi, stream;
   // packet range of this instance in the global packet index space

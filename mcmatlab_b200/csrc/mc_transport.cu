@@ -310,7 +310,13 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
             if (GRAD) P.inbox = in_box(*I, P.i);
           }
         }
-        if (++P.nsteps >= kMaxFreeSteps) P.alive = false;
+        if (++P.nsteps >= kMaxFreeSteps) {
+          P.alive = false;
+          if (!replay) {
+            atomicAdd(&I->ctr[4], 1ull);
+            atomicAdd(reinterpret_cast<double *>(&I->ctr[5]), (double)P.weight);
+          }
+        }
       }
     }
     // 4. scattering events in groups: a packet whose free path is used up waits (no sub-step)
@@ -522,6 +528,10 @@ std::vector<float> beam_cdf(const mcb_distr &d, bool radial) {
   return o;
 }
 
+// per-wavelength device counters: launched, collected, (unused), failed launches, free-step cuts
+// and their weight (FP64 bits)
+constexpr int kCtr = 6;
+
 struct ModelPlan {
   const mcb_mc_model *m;
   mcb_mc_result *r;
@@ -540,7 +550,7 @@ struct ModelPlan {
   float *beam = nullptr;     // FP1 | FP2 | AI1 | AI2
   double *S = nullptr;       // [nL][L+1]
   double *accNFR = nullptr, *accImg = nullptr, *accFF = nullptr, *accNI = nullptr;
-  unsigned long long *ctr = nullptr;  // [nL][4]
+  unsigned long long *ctr = nullptr;  // [nL][kCtr]
   long long Lim = 0, Lff = 0, Lx = 0, Ly = 0, Lz = 0, Lzn = 0, niPer = 0;
   std::vector<Inst> insts;   // one per wavelength
 };
@@ -741,13 +751,13 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
   if (pl.Lim) pl.accImg = ar.take<double>((size_t)pl.Lim * nL);
   if (pl.Lff) pl.accFF = ar.take<double>((size_t)pl.Lff * nL);
   pl.accNI = ar.take<double>((size_t)pl.niPer * nL);
-  pl.ctr = ar.take<unsigned long long>(4 * (size_t)nL);
+  pl.ctr = ar.take<unsigned long long>(kCtr * (size_t)nL);
   if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
   if (pl.accNFR) MCB_CUDA(ctx, cudaMemsetAsync(pl.accNFR, 0, 8 * (size_t)L * nL, st));
   if (pl.accImg) MCB_CUDA(ctx, cudaMemsetAsync(pl.accImg, 0, 8 * (size_t)pl.Lim * nL, st));
   if (pl.accFF) MCB_CUDA(ctx, cudaMemsetAsync(pl.accFF, 0, 8 * (size_t)pl.Lff * nL, st));
   MCB_CUDA(ctx, cudaMemsetAsync(pl.accNI, 0, 8 * (size_t)pl.niPer * nL, st));
-  MCB_CUDA(ctx, cudaMemsetAsync(pl.ctr, 0, 8 * 4 * (size_t)nL, st));
+  MCB_CUDA(ctx, cudaMemsetAsync(pl.ctr, 0, 8 * kCtr * (size_t)nL, st));
 
   // beam basis (MCmatlab.c:579-589)
   const double tb = pl.useS ? 0 : m->theta, pb = pl.useS ? 0 : m->phi, psib = pl.useS ? 0 : m->psi;
@@ -840,7 +850,7 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     } else if (m->boundaryType == 3) {
       I.NIzp = ni; I.NIzn = ni + pl.Lz;
     }
-    I.ctr = pl.ctr + 4 * iL;
+    I.ctr = pl.ctr + kCtr * iL;
     I.key0 = (uint32_t)m->seed;
     I.key1 = (uint32_t)(m->seed >> 32);
     I.ctr2hi = (uint32_t)iL << 16;
@@ -931,16 +941,21 @@ mcb_status finish_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, double *nPhCum, d
   const int nL = pl.nL;
   const long long L = pl.L;
   const int grid = ctx->num_sms * 8;
-  std::vector<unsigned long long> ctr(4 * (size_t)nL);
+  std::vector<unsigned long long> ctr(kCtr * (size_t)nL);
+  r->freeStepCuts = r->freeStepCutWeight = 0.0;
   MCB_CUDA(ctx, cudaMemcpyAsync(ctr.data(), pl.ctr, 8 * ctr.size(), cudaMemcpyDeviceToHost, st));
   MCB_CUDA(ctx, cudaStreamSynchronize(st));
   const double V = m->dx * m->dy * m->dz;
   float *stage = ar.take<float>(std::max<long long>(std::max<long long>(L, pl.Lim), std::max<long long>(pl.Lff, pl.niPer)));
   if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
   for (int iL = 0; iL < nL; iL++) {
-    const double nPh = (double)ctr[4 * iL], nCol = (double)ctr[4 * iL + 1];
+    const double nPh = (double)ctr[kCtr * iL], nCol = (double)ctr[kCtr * iL + 1];
     *nPhCum += nPh;
     *nColCum += nCol;
+    double cutW;
+    std::memcpy(&cutW, &ctr[kCtr * iL + 5], 8);
+    r->freeStepCuts += (double)ctr[kCtr * iL + 4];
+    r->freeStepCutWeight += cutW;
     // normfactor (MCmatlablib.c:1193-1198)
     double nf = nPh / pl.power[iL];
     if (pl.useS) nf /= pl.power[iL];
@@ -1078,7 +1093,7 @@ static mcb_status run_models(mcb_ctx *ctx, int n, const mcb_mc_model *const *mod
       MCB_TRY(launch_transport(ctx, ar, one, true, target, secs, &steps, &ms, &status));
       ar.used = mark;
       unsigned long long c[4];
-      MCB_CUDA(ctx, cudaMemcpy(c, pl.ctr + 4 * iL, 32, cudaMemcpyDeviceToHost));
+      MCB_CUDA(ctx, cudaMemcpy(c, pl.ctr + kCtr * iL, 32, cudaMemcpyDeviceToHost));
       colSoFar += (double)c[1];
       if (status & 1) break;
     }

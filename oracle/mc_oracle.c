@@ -77,6 +77,7 @@ typedef struct {
   /* accumulators */
   double *NFR, *image, *FF, *NIxp, *NIxn, *NIyp, *NIyn, *NIzp, *NIzn;
   unsigned long long nPhotons, nPhotonsCollected;
+  double cuts, cutW; /* packets ended by the free-step limit and their weight (all wavelengths) */
   unsigned long long steps;
   uint32_t key[2];
   uint32_t stream;
@@ -694,7 +695,13 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
         check_escape(R, P);
         if (P->alive) voxel_props(R, P);
       }
-      if (++P->psteps >= ORC_MAX_FREE_STEPS) P->alive = false;
+      if (++P->psteps >= ORC_MAX_FREE_STEPS) {
+        P->alive = false;
+#pragma omp atomic
+        R->cuts += 1.0;
+#pragma omp atomic
+        R->cutW += P->weight;
+      }
     }
     if (P->alive && P->weight < O_THRESHOLD) {
       if (rnd(R, P) <= O_CHANCE) P->weight /= O_CHANCE;
@@ -974,6 +981,8 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
   out->nThreads = nth;
   out->simulationTime = 0;
   out->propagationSteps = steps;
+  out->freeStepCuts = R.cuts;
+  out->freeStepCutWeight = R.cutW;
   out->examplePathsN = 0;
   free(M0); free(R.mua); free(R.mus); free(R.g); free(R.RI); free(R.cdfidx);
   free(R.FP1); free(R.FP2); free(R.AI1); free(R.AI2);

@@ -103,3 +103,33 @@ def ztest(batches_a, batches_b, zmax=4.5, rel_floor=0.0):
         if z > zmax:
             ok = False
     return ok, "\n".join(lines), worst
+
+
+def welch_z(ma, va, na, mb, vb, nb):
+    """Normal-equivalent z of the Welch t statistic for the difference of two batch means.
+
+    ma, mb: batch means; va, vb: batch variances (ddof 1); na, nb: batch counts. The Welch t
+    (unequal variances, Welch-Satterthwaite degrees of freedom) is mapped through its own
+    tail probability to the standard normal quantile with the same tail, so that under equal
+    means z is N(0, 1) for normal batch values whatever the batch counts: |z| > 3 then has the
+    normal 0.27% rate and mean(z^2) has expectation 1."""
+    from scipy import stats
+    ma, va, mb, vb = (np.asarray(x, dtype=np.float64) for x in (ma, va, mb, vb))
+    sa, sb = va / na, vb / nb
+    se2 = sa + sb
+    z = np.zeros(np.broadcast(ma, mb).shape)
+    ok = se2 > 0
+    t = np.where(ok, (ma - mb) / np.sqrt(np.where(ok, se2, 1.0)), 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        dof = se2 ** 2 / (sa ** 2 / (na - 1) + sb ** 2 / (nb - 1))
+    dof = np.where(ok & np.isfinite(dof), dof, 1e6)
+    p = stats.t.sf(np.abs(t), dof)
+    z = np.sign(t) * stats.norm.isf(np.clip(p, 1e-300, 0.5))
+    return np.where(ok, z, np.where(ma == mb, 0.0, np.inf))
+
+
+def voxel_chi2(ma, va, na, mb, vb, nb):
+    """Voxel-wise agreement of two batch-mean fields: (chi^2 / dof of the Welch z values,
+    fraction of voxels beyond 3 sigma, the z values)."""
+    z = welch_z(ma, va, na, mb, vb, nb)
+    return float(np.mean(z ** 2)), float(np.mean(np.abs(z) > 3.0)), z
