@@ -278,6 +278,8 @@ def run_ours(args):
         res["mc_grad"] = grad_measure(dev, args.c3_packets, args.c3_grid)
     if args.c4 and ws == 1:
         res["heat_adjoint"] = adjoint_measure(dev, args.c4_steps)
+    if args.lbfgs and ws == 1:
+        res["lbfgs"] = lbfgs_measure(dev, args.c3_packets, args.c3_grid)
     if rank == 0:
         if args.cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(args, sample_steps=args.ref_nt)
@@ -363,6 +365,27 @@ def adjoint_measure(dev, nt):
             "forward_voxel_updates_per_s": L * nt / (fwd_ms / 1e3), "forward_ms": fwd_ms,
             "adjoint_forward_sweep_ms": g["forwardMs"], "adjoint_reverse_sweep_ms": g["adjointMs"],
             "adjoint_over_forward": (g["forwardMs"] + g["adjointMs"]) / fwd_ms}
+
+
+def lbfgs_measure(dev, packets, n):
+    """Recovery of the top two tissue layers' mua and mus of the n^3 8-medium cube from its 32-bin
+    radial reflectance map (generated at the seeded ground truth with an independent seed and 2x
+    the packets) by L-BFGS over perturbation-MC gradients, from mua x 1.5, mus x 0.7."""
+    from mcmatlab_b200 import grad, native
+    mc_in = mexargs.prepare_mc(configs.perturbation_cube(n=n, nPhotons=packets))
+    obj = dict(nRadialBins=32, radialBinWidth=0.25 / 32, box=None)
+    ta = np.asarray(mc_in["mua"])[:, 0].copy()
+    ts = np.asarray(mc_in["mus"])[:, 0].copy()
+    media = [1, 2]
+    t0 = time.perf_counter()
+    _, g = native.mc_grad(dict(mc_in, seed=1001, nPhotonsRequested=2 * packets), device=dev, **obj)
+    r = grad.recover_optical_properties(mc_in, g["R"], media, obj, mua0=ta[media] * 1.5, mus0=ts[media] * 0.7,
+                                        max_evals=45)
+    return {"workload": "L-BFGS recovery of 2 layers' mua, mus on the %d^3 8-medium cube, %.0e packets per evaluation"
+                        % (n, packets), "evaluations": r["evals"], "seconds": time.perf_counter() - t0,
+            "relative_errors": {"mua": [float(r["mua"][m] / ta[m] - 1) for m in media],
+                                "mus": [float(r["mus"][m] / ts[m] - 1) for m in media]},
+            "final_loss": r["loss"]}
 
 
 REF_MC_PACKETS = 1e6
@@ -470,6 +493,7 @@ def main():
     ap.add_argument("--c3-grid", type=int, default=256)
     ap.add_argument("--no-c4", dest="c4", action="store_false", help="skip the heat-adjoint measurement")
     ap.add_argument("--c4-steps", type=int, default=2000)
+    ap.add_argument("--lbfgs", action="store_true", help="also run the L-BFGS recovery (about 80 s at 256^3, 1e8 packets)")
     ap.add_argument("--c4-cpu-steps", type=int, default=10, help="time steps of the CPU reference on the 300x300x200 grid")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -131,10 +131,31 @@ typedef struct mcb_mc_result {
    * the reference has no such limit) and their remaining weight, summed over wavelengths, in
    * units of one launched packet's weight */
   double freeStepCuts, freeStepCutWeight;
+  /* FP64 tallies before normalisation (no counterpart in the reference, whose MEX keeps them in
+   * thread-local memory and returns only normalised single-precision outputs). NULL = not
+   * wanted; else [mcb_mc_tally_count(model)] doubles, wavelength-major blocks of: the absorbed
+   * weight per voxel (when calcNFR), the light-collector image, the far field, the escape-face
+   * tallies, and last the launched and collected packet counts, 2 per wavelength. Tallies of runs
+   * of one model on disjoint packet ranges (packetOffset) add up to the tallies of their union;
+   * mcb_mc_normalize turns a sum into the outputs of that union. */
+  double *tallies;
 } mcb_mc_result;
 
 /* Replaces MCmatlab.c mexFunction: runs all wavelengths, normalises and writes the outputs. */
 MCB_API mcb_status mcb_mc_run(mcb_ctx *ctx, const mcb_mc_model *model, mcb_mc_result *result);
+
+/* No counterpart in the reference: number of doubles mcb_mc_result.tallies receives for model
+ * (0 for an invalid model). */
+MCB_API int64_t mcb_mc_tally_count(const mcb_mc_model *model);
+
+/* No counterpart in the reference: the normalisation of a run (normalizeDepositionAndResetO,
+ * MCmatlablib.c:1186-1250, as mcb_mc_run applies it) applied to given FP64 tallies, e.g. the sum
+ * of the tallies of several runs of model on disjoint packet ranges: writes the normalised
+ * outputs, nPhotons and nPhotonsCollected of result (its tallies field is ignored). The merged
+ * outputs equal those of one run over the union of the packets, up to FP64 summation order
+ * (combineModels.m:59-101 merges normalised single-precision outputs instead). */
+MCB_API mcb_status mcb_mc_normalize(mcb_ctx *ctx, const mcb_mc_model *model, const double *tallies,
+                                    mcb_mc_result *result);
 
 /* No counterpart in the reference: runs n independent models (different grids, media,
  * wavelengths, photon counts) in one persistent launch. Each model's packets use the random

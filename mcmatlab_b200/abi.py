@@ -62,6 +62,7 @@ class mcb_mc_result(C.Structure):
         ("simulationTime", C.c_double),
         ("propagationSteps", C.c_uint64), ("kernelMs", C.c_double),
         ("freeStepCuts", C.c_double), ("freeStepCutWeight", C.c_double),
+        ("tallies", _dp),
     ]
 
 
@@ -244,7 +245,7 @@ def result_shapes(mc_in):
 class McResultBuffers:
     """Output arrays sized as MCmatlab.c allocates them (:461-493), returned in MATLAB shapes."""
 
-    def __init__(self, mc_in, example_cap=0):
+    def __init__(self, mc_in, example_cap=0, tally_count=0):
         self.shapes = result_shapes(mc_in)
         self.arrays = {k: np.zeros(int(np.prod(s)), dtype=np.float32) for k, s in self.shapes.items()}
         r = mcb_mc_result()
@@ -253,6 +254,9 @@ class McResultBuffers:
         self.paths = np.zeros(4 * max(example_cap, 1), dtype=np.float64)
         r.examplePaths = _ptr(self.paths, C.c_double)
         r.examplePathsCap = example_cap
+        self.tallies = np.zeros(tally_count, dtype=np.float64) if tally_count else None
+        if tally_count:
+            r.tallies = _ptr(self.tallies, C.c_double)
         self.result = r
 
     def outputs(self):
@@ -266,6 +270,8 @@ class McResultBuffers:
         out["kernelMs"] = r.kernelMs
         out["freeStepCuts"] = r.freeStepCuts
         out["freeStepCutWeight"] = r.freeStepCutWeight
+        if self.tallies is not None:
+            out["tallies"] = self.tallies
         n = int(r.examplePathsN)
         out["examplePaths"] = self.paths[:4 * n].reshape(4, n, order="F") if n else np.zeros((4, 0))
         return out

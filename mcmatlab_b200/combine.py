@@ -134,3 +134,17 @@ def combineModels(modelArray, simType):
     else:
         raise ValueError("Error: simType must be 'MC' or 'FMC'")
     return out
+
+
+def merge_tallies(mc_in, runs, device=0):
+    """Exact merging of runs of one model (MEX-level inputs mc_in) on disjoint packet ranges, e.g.
+    a run continued later with packetOffset = the packets already run: the runs' FP64 tallies
+    (native.mc_run(..., tallies=True)) are added and normalised once (mcb_mc_normalize), which
+    gives the outputs of one run over the union of the packets up to FP64 summation order.
+    combineModels merges the runs' normalised single-precision outputs instead."""
+    from . import native
+    total = None
+    for r in runs:
+        t = np.asarray(r["tallies"], dtype=np.float64)
+        total = t.copy() if total is None else total + t
+    return native.mc_normalize(mc_in, total, device=device)

@@ -649,7 +649,7 @@ size_t plan_bytes(const mcb_mc_model *m) {
   if (m->farFieldRes) add(8 * (size_t)m->farFieldRes * m->farFieldRes * nL);
   const long long nx = m->nx, ny = m->ny, nz = m->nz;
   add(8 * (size_t)(2 * ny * nz + 2 * nx * nz + nx * ny + 25 * nx * ny) * nL);
-  add(8 * 4 * (size_t)nL);
+  add(8 * kCtr * (size_t)nL);
   add(sizeof(Inst) * nL + 8 * (nL + 1));
   // float staging for outputs
   size_t fo = 0;
@@ -662,6 +662,35 @@ size_t plan_bytes(const mcb_mc_model *m) {
 }
 
 // Copies inputs and builds the instance table of one model inside the arena.
+// Offsets (in doubles) of the blocks of mcb_mc_result.tallies; the accumulator sizes are those
+// build_plan gives the plan's device accumulators.
+struct TallyLayout {
+  long long nfr, img, ff, ni, cnt, total;
+};
+
+TallyLayout tally_layout(const mcb_mc_model *m) {
+  const long long nx = m->nx, ny = m->ny, nz = m->nz, L = nx * ny * nz, nL = m->nL;
+  const bool useS = m->sourceDistribution != nullptr;
+  const long long res = m->LC_res, nT = (!useS && m->LC_nTimeBins) ? m->LC_nTimeBins + 2 : 1;
+  const long long Lim = m->useLightCollector ? res * res * nT : 0, Lff = (long long)m->farFieldRes * m->farFieldRes;
+  const long long Lzn = m->boundaryType == 2 ? nx * ny * kKillRange * kKillRange : nx * ny;
+  const long long niPer = 2 * ny * nz + 2 * nx * nz + nx * ny + Lzn;
+  TallyLayout t;
+  long long o = 0;
+  t.nfr = o;
+  o += m->calcNFR ? L * nL : 0;
+  t.img = o;
+  o += Lim * nL;
+  t.ff = o;
+  o += Lff * nL;
+  t.ni = o;
+  o += niPer * nL;
+  t.cnt = o;
+  o += 2 * nL;
+  t.total = o;
+  return t;
+}
+
 mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
   const mcb_mc_model *m = pl.m;
   cudaStream_t st = ctx->stream;
@@ -944,7 +973,22 @@ mcb_status finish_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, double *nPhCum, d
   std::vector<unsigned long long> ctr(kCtr * (size_t)nL);
   r->freeStepCuts = r->freeStepCutWeight = 0.0;
   MCB_CUDA(ctx, cudaMemcpyAsync(ctr.data(), pl.ctr, 8 * ctr.size(), cudaMemcpyDeviceToHost, st));
+  if (r->tallies) {
+    // the FP64 tallies as accumulated (the normalisation below reads them, it does not change them)
+    const TallyLayout t = tally_layout(m);
+    if (pl.accNFR) MCB_CUDA(ctx, cudaMemcpyAsync(r->tallies + t.nfr, pl.accNFR, 8 * (size_t)L * nL, cudaMemcpyDeviceToHost, st));
+    if (pl.accImg) MCB_CUDA(ctx, cudaMemcpyAsync(r->tallies + t.img, pl.accImg, 8 * (size_t)pl.Lim * nL, cudaMemcpyDeviceToHost, st));
+    if (pl.accFF) MCB_CUDA(ctx, cudaMemcpyAsync(r->tallies + t.ff, pl.accFF, 8 * (size_t)pl.Lff * nL, cudaMemcpyDeviceToHost, st));
+    MCB_CUDA(ctx, cudaMemcpyAsync(r->tallies + t.ni, pl.accNI, 8 * (size_t)pl.niPer * nL, cudaMemcpyDeviceToHost, st));
+  }
   MCB_CUDA(ctx, cudaStreamSynchronize(st));
+  if (r->tallies) {
+    const TallyLayout t = tally_layout(m);
+    for (int iL = 0; iL < nL; iL++) {
+      r->tallies[t.cnt + 2 * iL] = (double)ctr[kCtr * iL];
+      r->tallies[t.cnt + 2 * iL + 1] = (double)ctr[kCtr * iL + 1];
+    }
+  }
   const double V = m->dx * m->dy * m->dz;
   float *stage = ar.take<float>(std::max<long long>(std::max<long long>(L, pl.Lim), std::max<long long>(pl.Lff, pl.niPer)));
   if (ar.overflow) return set_error(ctx, MCB_ENOMEM, "internal: device arena too small");
@@ -1199,6 +1243,57 @@ extern "C" mcb_status mcb_mc_grad(mcb_ctx *ctx, const mcb_mc_model *model, const
   const mcb_mc_model *ms[1] = {model};
   mcb_mc_result *rs[1] = {result};
   return run_models(ctx, 1, ms, rs, objectives, grad);
+}
+
+extern "C" int64_t mcb_mc_tally_count(const mcb_mc_model *model) {
+  if (!model || model->nx < 1 || model->ny < 1 || model->nz < 1 || model->nL < 1) return 0;
+  return tally_layout(model).total;
+}
+
+extern "C" mcb_status mcb_mc_normalize(mcb_ctx *ctx, const mcb_mc_model *model, const double *tallies,
+                                       mcb_mc_result *result) {
+  using namespace mcb;
+  if (!ctx) return MCB_EINVAL;
+  MCB_TRY(validate(ctx, model));
+  if (!tallies || !result) return set_error(ctx, MCB_EINVAL, "tallies or result is NULL");
+  MCB_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = (1 << 20) + plan_bytes(model) + (size_t)(sizeof(Inst) + 16) * 64;
+  void *base = nullptr;
+  MCB_TRY(pool_get(ctx, SLOT_MC_INST, bytes, &base));
+  Arena ar{(char *)base, bytes, 0};
+  ModelPlan pl;
+  pl.m = model;
+  pl.r = result;
+  MCB_TRY(build_plan(ctx, ar, pl, 0));
+  const TallyLayout t = tally_layout(model);
+  const int nL = model->nL;
+  cudaStream_t st = ctx->stream;
+  if (pl.accNFR) MCB_CUDA(ctx, cudaMemcpyAsync(pl.accNFR, tallies + t.nfr, 8 * (size_t)pl.L * nL, cudaMemcpyHostToDevice, st));
+  if (pl.accImg) MCB_CUDA(ctx, cudaMemcpyAsync(pl.accImg, tallies + t.img, 8 * (size_t)pl.Lim * nL, cudaMemcpyHostToDevice, st));
+  if (pl.accFF) MCB_CUDA(ctx, cudaMemcpyAsync(pl.accFF, tallies + t.ff, 8 * (size_t)pl.Lff * nL, cudaMemcpyHostToDevice, st));
+  MCB_CUDA(ctx, cudaMemcpyAsync(pl.accNI, tallies + t.ni, 8 * (size_t)pl.niPer * nL, cudaMemcpyHostToDevice, st));
+  std::vector<unsigned long long> c(kCtr * (size_t)nL, 0ull);
+  for (int iL = 0; iL < nL; iL++) {
+    const double a = tallies[t.cnt + 2 * iL], b = tallies[t.cnt + 2 * iL + 1];
+    if (!(a >= 0 && b >= 0 && a < 1.8e19 && b < 1.8e19)) return set_error(ctx, MCB_EINVAL, "packet counts out of range");
+    c[kCtr * iL] = (unsigned long long)a;
+    c[kCtr * iL + 1] = (unsigned long long)b;
+  }
+  MCB_CUDA(ctx, cudaMemcpyAsync(pl.ctr, c.data(), 8 * c.size(), cudaMemcpyHostToDevice, st));
+  double *keep = result->tallies;
+  result->tallies = nullptr;
+  double nPh = 0, nCol = 0;
+  const mcb_status rc = finish_plan(ctx, ar, pl, &nPh, &nCol);
+  result->tallies = keep;
+  MCB_TRY(rc);
+  result->nPhotons = nPh;
+  result->nPhotonsCollected = nCol;
+  result->nThreads = 0;
+  result->simulationTime = 0;
+  result->propagationSteps = 0;
+  result->kernelMs = 0;
+  result->examplePathsN = 0;
+  return MCB_OK;
 }
 
 extern "C" mcb_status mcb_mc_run_batch(mcb_ctx *ctx, int32_t n, const mcb_mc_model *const *models,

@@ -27,7 +27,7 @@ EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_fl
            "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint", "mcb_probe_atomics",
            "mcb_interface_normals", "mcb_downsample_params",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
-           "mcb_heat_state_destroy", "mcb_last_kernel_ms")
+           "mcb_heat_state_destroy", "mcb_last_kernel_ms", "mcb_mc_tally_count", "mcb_mc_normalize")
 
 
 class MCBError(RuntimeError):
@@ -73,6 +73,10 @@ def lib():
                                                 C.c_double, C.c_double, C.POINTER(C.c_float)]
             L.mcb_downsample_params.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.c_int64, C.c_int32,
                                                 C.POINTER(C.c_float), C.POINTER(C.c_uint8)]
+            L.mcb_mc_tally_count.argtypes = [C.POINTER(abi.mcb_mc_model)]
+            L.mcb_mc_tally_count.restype = C.c_int64
+            L.mcb_mc_normalize.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.POINTER(C.c_double),
+                                           C.POINTER(abi.mcb_mc_result)]
             L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
             L.mcb_last_kernel_ms.restype = C.c_double
             _lib = L
@@ -96,12 +100,29 @@ def _check(st, ctx):
         raise MCBError(st, lib().mcb_last_error(ctx).decode())
 
 
-def mc_run(mc_in, device=0, example_cap=100000):
-    """Runs one model (MEX-level inputs from mexargs.prepare_mc); returns outputs in MATLAB shapes."""
+def mc_run(mc_in, device=0, example_cap=100000, tallies=False):
+    """Runs one model (MEX-level inputs from mexargs.prepare_mc); returns outputs in MATLAB shapes.
+    With tallies=True the output also holds "tallies": the run's FP64 tallies before
+    normalisation (mcb_mc_result.tallies), which add up over runs on disjoint packet ranges."""
     ctx = context(device)
     mb = abi.McModelBuffers(mc_in)
-    rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0)
+    nt = int(lib().mcb_mc_tally_count(C.byref(mb.model))) if tallies else 0
+    rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0, nt)
     _check(lib().mcb_mc_run(ctx, C.byref(mb.model), C.byref(rb.result)), ctx)
+    return rb.outputs()
+
+
+def mc_normalize(mc_in, tallies, device=0):
+    """Normalised outputs (MATLAB shapes, nPhotons, nPhotonsCollected) of given FP64 tallies of
+    model mc_in, e.g. the sum of the "tallies" of runs on disjoint packet ranges: the outputs of
+    one run over the union of their packets (mcb_mc_normalize)."""
+    ctx = context(device)
+    mb = abi.McModelBuffers(mc_in)
+    t = np.ascontiguousarray(np.asarray(tallies, dtype=np.float64))
+    if t.size != int(lib().mcb_mc_tally_count(C.byref(mb.model))):
+        raise ValueError("tallies have %d entries, the model needs %d" % (t.size, lib().mcb_mc_tally_count(C.byref(mb.model))))
+    rb = abi.McResultBuffers(mc_in)
+    _check(lib().mcb_mc_normalize(ctx, C.byref(mb.model), t.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rb.result)), ctx)
     return rb.outputs()
 
 

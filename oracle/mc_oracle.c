@@ -78,6 +78,11 @@ typedef struct {
   double *NFR, *image, *FF, *NIxp, *NIxn, *NIyp, *NIyn, *NIzp, *NIzn;
   unsigned long long nPhotons, nPhotonsCollected;
   double cuts, cutW; /* packets ended by the free-step limit and their weight (all wavelengths) */
+  /* example-path recording (one thread, packets 0, 1, 2, ... of the first wavelength): columns of
+   * (x, y, z, weight), NaN-separated (MCmatlablib.c:465-514); pn > pcap marks an overflow */
+  double *pdata;
+  long pcap, pn;
+  int pstarted;
   unsigned long long steps;
   uint32_t key[2];
   uint32_t stream;
@@ -584,8 +589,10 @@ static void edge_fluxes(orc_mc *R, const orc_photon *P) {
   }
 }
 
-static void check_escape(orc_mc *R, orc_photon *P) {
+/* Returns whether the packet was wrapped to the opposite face (cyclic boundaries). */
+static int check_escape(orc_mc *R, orc_photon *P) {
   bool esc = false;
+  int tele = 0;
   const double h = O_KILLRANGE / 2.0;
   const long *n = R->n;
   switch (R->bt) {
@@ -604,10 +611,10 @@ static void check_escape(orc_mc *R, orc_photon *P) {
       bool tooOld = P->time > 1000 / O_C * sqrt(sqr(R->d[0] * n[0]) + sqr(R->d[1] * n[1]));
       P->alive = P->i[2] < n[2] && P->i[2] >= 0 && !tooOld;
       esc = !P->alive && P->RI == 1 && !tooOld;
-      if (P->i[0] >= n[0]) P->i[0] = 0;
-      if (P->i[0] < 0) P->i[0] = n[0] * (1 - DBL_EPSILON);
-      if (P->i[1] >= n[1]) P->i[1] = 0;
-      if (P->i[1] < 0) P->i[1] = n[1] * (1 - DBL_EPSILON);
+      if (P->i[0] >= n[0]) { P->i[0] = 0; tele = 1; }
+      if (P->i[0] < 0) { P->i[0] = n[0] * (1 - DBL_EPSILON); tele = 1; }
+      if (P->i[1] >= n[1]) { P->i[1] = 0; tele = 1; }
+      if (P->i[1] < 0) { P->i[1] = n[1] * (1 - DBL_EPSILON); tele = 1; }
       break;
     }
   }
@@ -635,6 +642,7 @@ static void check_escape(orc_mc *R, orc_photon *P) {
       }
     }
   }
+  return tele;
 }
 
 static void scatter(orc_mc *R, orc_photon *P) {
@@ -676,6 +684,31 @@ static void scatter(orc_mc *R, orc_photon *P) {
  * has no limit) */
 #define ORC_MAX_FREE_STEPS 20000UL
 
+/* addToPhotonPath (MCmatlablib.c:479-504): nanCols NaN columns, then the packet's position and
+ * weight */
+static void path_add(orc_mc *R, const orc_photon *P, int nanCols) {
+  if (R->pn + nanCols + 1 > R->pcap) {
+    R->pn = R->pcap + 1;
+    return;
+  }
+  for (int c = 0; c < nanCols; c++) {
+    for (int r = 0; r < 4; r++) R->pdata[4 * R->pn + r] = NAN;
+    R->pn++;
+  }
+  R->pdata[4 * R->pn + 0] = (P->i[0] - R->n[0] / 2.0) * R->d[0];
+  R->pdata[4 * R->pn + 1] = (P->i[1] - R->n[1] / 2.0) * R->d[1];
+  R->pdata[4 * R->pn + 2] = P->i[2] * R->d[2];
+  R->pdata[4 * R->pn + 3] = P->weight;
+  R->pn++;
+  R->pstarted = 1;
+}
+
+/* updatePaths (MCmatlablib.c:507-514); a no-op outside example-path recording */
+static void path_update(orc_mc *R, orc_photon *P, int teleported) {
+  if (!R->pdata || R->pn > R->pcap) return;
+  if (R->eol || criteria(R, P)) path_add(R, P, R->pstarted ? (teleported ? 1 : 0) : 2);
+}
+
 static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
   P->pid = pid;
   P->draw = 0;
@@ -684,6 +717,7 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
   P->psteps = 0;
   for (int m = 0; m < 10; m++) P->L[m] = P->k[m] = 0.0;
   if (P->alive) {
+    path_update(R, P, 0);
     voxel_props(R, P);
 #pragma omp atomic
     R->nPhotons++;
@@ -691,8 +725,9 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
   while (P->alive) {
     while (P->alive && P->stepLeft > 0) {
       propagate(R, P);
+      path_update(R, P, 0);
       if (!P->sameVoxel) {
-        check_escape(R, P);
+        if (check_escape(R, P) && (R->eol || criteria(R, P))) path_update(R, P, 1);
         if (P->alive) voxel_props(R, P);
       }
       if (++P->psteps >= ORC_MAX_FREE_STEPS) {
@@ -710,10 +745,36 @@ static void run_packet(orc_mc *R, orc_photon *P, uint64_t pid) {
     if (P->alive) {
       P->psteps = 0;
       scatter(R, P);
+      path_update(R, P, 0);
     }
   }
   if (R->eol && criteria(R, P) && R->NFR)
     for (long k = 0; k < P->recN; k++) add(&R->NFR[P->jrec[k]], P->weight * P->wrec[k]);
+}
+
+/* Example paths: packets 0, 1, 2, ... (of the unsharded stream) replayed one after another with
+ * their vertices recorded, until nPaths paths are finished (MCmatlab.c:270-278: a path whose
+ * end-of-life criteria fail is deleted). Tallies the replay makes are the caller's to discard. */
+static long record_paths(orc_mc *R, long nPaths, uint64_t maxP, double *data, long cap) {
+  orc_photon P;
+  memset(&P, 0, sizeof P);
+  R->pdata = data;
+  R->pcap = cap;
+  R->pn = 0;
+  long finished = 0;
+  for (uint64_t pid = 0; pid < maxP && finished < nPaths && R->pn <= cap; pid++) {
+    const long startN = R->pn;
+    R->pstarted = 0;
+    run_packet(R, &P, pid);
+    if (R->pstarted) {
+      if (R->eol && !criteria(R, &P)) R->pn = startN;
+      else finished++;
+    }
+  }
+  free(P.jrec);
+  free(P.wrec);
+  R->pdata = NULL;
+  return R->pn > cap ? cap : R->pn;
 }
 
 static unsigned long infcast(double x) { return isinf(x) ? ULONG_MAX : (unsigned long)x; }
@@ -853,6 +914,7 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
   int nth = 1;
   (void)nthreads;
 #endif
+  out->examplePathsN = 0;
   for (int iL = 0; iL < nL; iL++) {
     for (int m = 0; m < in->nM; m++) {
       R.mua[m] = in->mua[m + (long)iL * in->nM];
@@ -950,6 +1012,25 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
     NORM(R.NIzp, out->NI_zpos, Lz, in->dx * in->dy)
     NORM(R.NIzn, out->NI_zneg, Lzn, in->dx * in->dy)
 #undef NORM
+    if (iL == 0 && in->nExamplePaths > 0 && out->examplePaths && out->examplePathsCap > 0 && !R.grad) {
+      const unsigned long long nPh0 = R.nPhotons, nCol0 = R.nPhotonsCollected;
+      const double cuts0 = R.cuts, cutW0 = R.cutW;
+      out->examplePathsN = record_paths(&R, (long)in->nExamplePaths, nPh0, out->examplePaths, (long)out->examplePathsCap);
+      /* discard the replay's tallies and counts */
+      if (R.NFR) memset(R.NFR, 0, sizeof(double) * L);
+      if (R.image) memset(R.image, 0, sizeof(double) * Lim);
+      if (R.FF) memset(R.FF, 0, sizeof(double) * Lff);
+      if (R.NIxp) memset(R.NIxp, 0, 8 * Lx);
+      if (R.NIxn) memset(R.NIxn, 0, 8 * Lx);
+      if (R.NIyp) memset(R.NIyp, 0, 8 * Ly);
+      if (R.NIyn) memset(R.NIyn, 0, 8 * Ly);
+      if (R.NIzp) memset(R.NIzp, 0, 8 * Lz);
+      if (R.NIzn) memset(R.NIzn, 0, 8 * Lzn);
+      R.nPhotons = nPh0;
+      R.nPhotonsCollected = nCol0;
+      R.cuts = cuts0;
+      R.cutW = cutW0;
+    }
     if (R.aborting) break;
   }
   if (R.grad && gres) {
@@ -983,7 +1064,6 @@ static int mc_run_impl(const mcb_mc_model *in, mcb_mc_result *out, int nthreads,
   out->propagationSteps = steps;
   out->freeStepCuts = R.cuts;
   out->freeStepCutWeight = R.cutW;
-  out->examplePathsN = 0;
   free(M0); free(R.mua); free(R.mus); free(R.g); free(R.RI); free(R.cdfidx);
   free(R.FP1); free(R.FP2); free(R.AI1); free(R.AI2);
   free(R.NFR); free(R.image); free(R.FF);

@@ -74,9 +74,11 @@ def oracle_downsample(paramVals, nBins):
     return out, idx
 
 
-def oracle_mc(mc_in, nthreads=0):
+def oracle_mc(mc_in, nthreads=0, example_cap=100000):
+    """FP64 transport on MEX-level inputs; with nExamplePaths > 0 also the example paths (packets
+    0, 1, 2, ... replayed one after another, as the CUDA path records them)."""
     mb = abi.McModelBuffers(mc_in)
-    rb = abi.McResultBuffers(mc_in)
+    rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0)
     rc = lib().orc_mc_run(C.byref(mb.model), C.byref(rb.result), int(nthreads))
     if rc != 0:
         raise RuntimeError("oracle MC run failed (%d)" % rc)

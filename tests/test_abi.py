@@ -47,3 +47,26 @@ def test_python_context_raises_without_gpu():
         native.context(0)
     with pytest.raises(native.MCBError):
         native.context(0)
+
+
+@pytest.mark.parametrize("name", ["c0_small", "radial_lens_ff", "broadband", "plane_bt2", "xy_custom_fiber_cyclic"])
+def test_tally_count_layout(name):
+    """mcb_mc_tally_count (host only, no GPU): per wavelength the voxel tallies, image, far field
+    and escape-face tallies (boundaryType 2: a 5x-wide z < 0 face), then two packet counts."""
+    import sys
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import mccases
+    from mcmatlab_b200 import abi, mexargs, native
+    mc_in = mexargs.prepare_mc(mccases.CASES[name]())
+    mb = abi.McModelBuffers(mc_in)
+    m = mb.model
+    nx, ny, nz, nL = m.nx, m.ny, m.nz, m.nL
+    nT = m.LC_nTimeBins + 2 if m.LC_nTimeBins else 1
+    Lim = m.LC_res ** 2 * nT if m.useLightCollector else 0
+    Lzn = 25 * nx * ny if m.boundaryType == 2 else nx * ny
+    per = (nx * ny * nz if m.calcNFR else 0) + Lim + m.farFieldRes ** 2 + 2 * ny * nz + 2 * nx * nz + nx * ny + Lzn + 2
+    assert native.lib().mcb_mc_tally_count(C.byref(m)) == per * nL
+    shapes = abi.result_shapes(mc_in)
+    if "NFR" in shapes:
+        assert int(np.prod(shapes["NFR"])) == nx * ny * nz * nL
