@@ -476,6 +476,37 @@ def run_reference(args):
     print(json.dumps(res), flush=True)
 
 
+def run_profile(args):
+    """Short runs of one workload for profiler captures (no JSON line; times printed for reference):
+    heat-c1: the heat state of the 100^3 cube stepped args.nt steps (source from a 1e5-packet run);
+    heat-c4: the 300x300x200 heat-adjoint grid stepped args.nt steps forward; mc-c0: the transport of
+    the 100^3 cube at args.packets packets; each args.steps times."""
+    from mcmatlab_b200 import native
+    if args.profile == "mc-c0":
+        mc_in = mexargs.prepare_mc(configs.standard_tissue_cube(n=N_GRID, nPhotons=args.packets, seed=1))
+        for _ in range(args.steps):
+            o = native.mc_run(mc_in)
+            print("mc-c0: %.0f packets in %.3f ms" % (args.packets, o["kernelMs"]), flush=True)
+        return
+    if args.profile == "heat-c1":
+        m = configs.standard_tissue_cube(n=N_GRID, nPhotons=1e5, seed=1)
+        mc_in = mexargs.prepare_mc(m)
+        out = native.mc_run(mc_in)
+        NA = mc_in["mua"][:, 0][mc_in["M"].astype(np.int64) - 1].astype(np.float32) * out["NFR"][..., 0]
+        th, c, Q, dt = build_heat_inputs(NA, m)
+        hp = mexargs.heat_mex_params(th["M"], th["A"], th["E"], c, Q, True, 0, None, None, True, args.nt, dt)
+        n = (N_GRID,) * 3
+        T0, O0 = np.full(n, 37.0, np.float32, order="F"), np.zeros(n, np.float32, order="F")
+    else:
+        case = configs.heat_adjoint_case(nt=args.nt)
+        n, hp, T0, O0 = case["n"], case["hp"], case["T0"], None
+    st = native.HeatState(T0, O0, hp, *n)
+    for _ in range(args.steps):
+        st.step(hp)
+        print("%s: %d steps in %.3f ms" % (args.profile, args.nt, native.last_kernel_ms(0)), flush=True)
+    st.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -495,9 +526,14 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--lbfgs", action="store_true", help="also run the L-BFGS recovery (about 80 s at 256^3, 1e8 packets)")
     ap.add_argument("--c4-cpu-steps", type=int, default=10, help="time steps of the CPU reference on the 300x300x200 grid")
+    ap.add_argument("--profile", choices=["heat-c1", "heat-c4", "mc-c0"], default=None,
+                    help="run one workload briefly for a profiler capture instead of the benchmark")
+    ap.add_argument("--packets", type=float, default=1e5, help="packets of the mc-c0 profile run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

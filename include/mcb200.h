@@ -157,6 +157,29 @@ MCB_API int64_t mcb_mc_tally_count(const mcb_mc_model *model);
 MCB_API mcb_status mcb_mc_normalize(mcb_ctx *ctx, const mcb_mc_model *model, const double *tallies,
                                     mcb_mc_result *result);
 
+/* No counterpart in the reference, which sizes its launch with cudaOccupancyMaxPotentialBlockSize
+ * (MCmatlab.c:641): the transport kernel's warp-grouping parameters. refillMin: a warp launches
+ * new packets on its free lanes once at least this many lanes are free; scatterMin: packets whose
+ * free path ran out wait until this many lanes of their warp are waiting before roulette and
+ * scattering run (both 1..32). Results do not depend on them (each packet's random stream is
+ * fixed); only the time does. */
+typedef struct mcb_mc_launch {
+  int32_t refillMin, scatterMin;
+} mcb_mc_launch;
+
+/* No counterpart in the reference: the launch-parameter class of a model (its voxel count in
+ * powers of 4; +16 for gradient runs, +32 for batches). */
+MCB_API int32_t mcb_mc_size_class(const mcb_mc_model *model, int32_t gradient, int32_t batched);
+
+/* No counterpart in the reference: autotuner. Runs `model` with calibrationPackets packets for
+ * every (refillMin, scatterMin) in {4, 8, 12, 16}^2 (twice each), keeps the fastest for the
+ * model's size class in this context (later runs of that class use it), and, when the environment
+ * variable MCB_TUNE_FILE names a file, records it there for this GPU model; contexts created later
+ * read that file. Writes the choice to *chosen and, when table is not NULL, the 16 candidates as
+ * rows {refillMin, scatterMin, best kernel ms} to table[48]. */
+MCB_API mcb_status mcb_mc_autotune(mcb_ctx *ctx, const mcb_mc_model *model, double calibrationPackets, int32_t gradient,
+                                   mcb_mc_launch *chosen, double *table);
+
 /* No counterpart in the reference: runs n independent models (different grids, media,
  * wavelengths, photon counts) in one persistent launch. Each model's packets use the random
  * streams of its own seed, so results equal n calls of mcb_mc_run up to FP64 summation order.

@@ -66,6 +66,10 @@ class mcb_mc_result(C.Structure):
     ]
 
 
+class mcb_mc_launch(C.Structure):
+    _fields_ = [("refillMin", C.c_int32), ("scatterMin", C.c_int32)]
+
+
 class mcb_mc_objectives(C.Structure):
     _fields_ = [("nRadialBins", C.c_int32), ("radialBinWidth", C.c_double), ("box", C.c_int32 * 6)]
 

@@ -63,6 +63,11 @@ extern "C" mcb_status mcb_ctx_create(int device, mcb_ctx **out) {
     return MCB_ECUDA;
   }
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) ctx->gpuName = prop.name;
+    mcb::tune_file_load(ctx);
+  }
   int *h = nullptr;
   if (cudaHostAlloc((void **)&h, sizeof(int) * 4, cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer((void **)&ctx->cancel_dev, h, 0) != cudaSuccess) {

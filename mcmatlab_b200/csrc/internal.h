@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -29,6 +30,11 @@ struct mcb_ctx {
   int num_sms = 0;
   mcb_heat_state *heat = nullptr;  // state reused by mcb_heat_forward
   double lastKernelMs = 0.0;        // device time of the last stepping / transport loop
+  // transport launch parameters: tuned per size class (mcb_mc_autotune, or read from the tuning
+  // file at context creation), and an override used while the autotuner calibrates
+  std::string gpuName;
+  std::map<int, mcb_mc_launch> tuned;
+  mcb_mc_launch force{0, 0};
 };
 
 namespace mcb {
@@ -37,6 +43,9 @@ mcb_status set_error(mcb_ctx *ctx, mcb_status st, const char *fmt, ...);
 
 // Returns a device buffer for `slot` of at least `bytes` (contents undefined).
 mcb_status pool_get(mcb_ctx *ctx, int slot, size_t bytes, void **out);
+
+// Reads the transport launch parameters tuned for this GPU from the file MCB_TUNE_FILE names.
+void tune_file_load(mcb_ctx *ctx);
 
 #define MCB_CUDA(ctx, call)                                                                      \
   do {                                                                                           \

@@ -101,6 +101,7 @@ struct Photon {
   float stepLeft, weight, time;
   bool inside, alive, sameVoxel;
   int med;   // medium of the current voxel
+  int jn, mn;  // voxel and medium entered by the last boundary-crossing sub-step (propagate)
   bool inbox;  // current voxel inside the gradient target box
   uint32_t scat, refr, refl, itr;
   uint32_t nsteps;  // propagation sub-steps since launch or the last scattering event
@@ -226,15 +227,29 @@ __device__ __forceinline__ void direction_changed(Photon &P, const Inst &I) {
   }
 }
 
-__device__ __forceinline__ void voxel_props(Photon &P, const Inst &I) {
-  P.j = voxel_index(I, P.i);
-  const int m = __ldg(I.M0 + P.j);
+__device__ __forceinline__ void medium_props(Photon &P, const Inst &I, int m) {
   P.med = m;
   const float4 mp = I.med[m];
   P.mua = mp.x;
   P.mus = mp.y;
   P.g = mp.z;
   P.cdf = I.cdfidx[m];
+}
+
+__device__ __forceinline__ void voxel_props(Photon &P, const Inst &I) {
+  P.j = voxel_index(I, P.i);
+  medium_props(P, I, __ldg(I.M0 + P.j));
+}
+
+// After a boundary-crossing sub-step and check_escape: the voxel and medium propagate already
+// looked up, unless the packet was wrapped to the opposite face (then looked up again).
+__device__ __forceinline__ void voxel_props_crossed(Photon &P, const Inst &I, bool teleported) {
+  if (teleported) {
+    voxel_props(P, I);
+  } else {
+    P.j = P.jn;
+    medium_props(P, I, P.mn);
+  }
 }
 
 __device__ __forceinline__ float launch_time(const Photon &P, const Inst &I, const float *t) {
@@ -485,6 +500,8 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
   if (!P.sameVoxel) {
     const int jn = voxel_index(I, P.i);
     const int mn = __ldg(I.M0 + jn);
+    P.jn = jn;
+    P.mn = mn;
     const float rin = I.med[mn].w;
     const float mu = P.RI / rin;
     if (mu != 1.f) {
@@ -517,7 +534,7 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
         }
       }
     } else {
-      const int mo = __ldg(I.M0 + P.j);
+      const int mo = P.med;  // medium of the voxel left (voxel_props)
       if (mn != mo && I.med[mo].w == P.RI && (uint32_t)mn >= I.minIdx && (uint32_t)mn <= I.maxIdx) P.itr++;
     }
   }

@@ -44,7 +44,8 @@ struct KernelArgs {
   unsigned long long *steps;
   // Refill threshold: a warp re-launches free lanes only when at least this many are free (or
   // none is alive), so the divergent launch code runs once for a group of lanes.
-  int refillMin;
+  int refillMin;   // free lanes a warp waits for before launching new packets
+  int scatterMin;  // waiting lanes before roulette + scattering run
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
           }
         }
         if (!P.sameVoxel) {
-          check_escape(P, *I, !replay);
+          const bool tele = check_escape(P, *I, !replay);
           if (GRAD && !P.alive && P.kec != 0 && P.i[2] < 0 && nGR > 0) {
             // reflectance: escaping weight W on the top face, d/dmua_m = -L_m W,
             // d/dmus_m = (k_m / mus_m - L_m) W
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
             }
           }
           if (P.alive) {
-            voxel_props(P, *I);
+            voxel_props_crossed(P, *I, tele);
             if (GRAD) P.inbox = in_box(*I, P.i);
           }
         }
@@ -322,15 +323,14 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
     // 4. scattering events in groups: a packet whose free path is used up waits (no sub-step)
     //    until enough lanes of its warp are waiting too, or no lane can take a sub-step, so the
     //    long scattering code runs with most lanes active. A packet's events and random draws do
-    //    not change, only when its warp performs them. Measured on the 100^3 cube / 256^3
-    //    8-medium cube: groups of 8 gave the plain kernel 9.5% / 6% more packets/s, groups of 16
-    //    the gradient kernel 4.5%.
+    //    not change, only when its warp performs them. The group size (a.scatterMin) is a launch
+    //    parameter of the autotuner; against single-lane scattering, groups of 8 gave the plain
+    //    kernel 9.5% more packets/s on the 100^3 cube.
     {
-      constexpr int kScatterGroup = GRAD ? 16 : 8;
       const bool want = P.alive && !(P.stepLeft > 0);
       const unsigned waiting = __ballot_sync(0xffffffffu, want);
       const unsigned stepping = __ballot_sync(0xffffffffu, P.alive && P.stepLeft > 0);
-      if (want && (__popc(waiting) >= kScatterGroup || stepping == 0)) {
+      if (want && (__popc(waiting) >= a.scatterMin || stepping == 0)) {
         if (P.weight < kThreshold) {
           if (rnd(P, *I) <= kChance) P.weight /= kChance;
           else P.alive = false;
@@ -442,7 +442,7 @@ __global__ void example_paths_kernel(const Inst *inst, int nPaths, unsigned long
         if (!P.sameVoxel) {
           const bool tele = check_escape(P, I, false);
           if (tele && (I.eol || criteria_met(P, I))) path_update(W, P, I, true);
-          if (P.alive) voxel_props(P, I);
+          if (P.alive) voxel_props_crossed(P, I, tele);
         }
         if (++P.nsteps >= kMaxFreeSteps) P.alive = false;
       }
@@ -900,6 +900,23 @@ size_t grad_smem_bytes(int nM, int nR, int threads) {
   return 8 * (size_t)(nR * (1 + 2 * nM) + 1 + 2 * nM) + 4 * (size_t)threads * (4 * nM + 1 + 2 * nM);
 }
 
+// Launch-parameter class: voxels in powers of 4 (0..15), +16 gradient, +32 batched.
+int size_class(long long voxels, bool grad, bool batched) {
+  int c = 0;
+  while (c < 15 && (1ll << (2 * (c + 1))) <= voxels) c++;
+  return c + (grad ? 16 : 0) + (batched ? 32 : 0);
+}
+
+// The autotuner's override, else the class's tuned parameters, else the autotuner's choices on the
+// 100^3 cube (refill 16, scatter 8: 6.83 ms for 1e6 packets against 7.14 ms at 8, 8) and on the
+// 256^3 gradient cube (12, 12).
+mcb_mc_launch launch_params(const mcb_ctx *ctx, int cls, bool grad) {
+  if (ctx->force.refillMin > 0) return ctx->force;
+  const auto it = ctx->tuned.find(cls);
+  if (it != ctx->tuned.end()) return it->second;
+  return grad ? mcb_mc_launch{12, 12} : mcb_mc_launch{16, 8};
+}
+
 mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &insts, bool openEnded,
                             unsigned long long collectTarget, double seconds, unsigned long long *stepsOut,
                             float *msOut, int *statusOut, bool grad = false) {
@@ -928,8 +945,13 @@ mcb_status launch_transport(mcb_ctx *ctx, Arena &ar, const std::vector<Inst> &in
   a.collectTarget = collectTarget;
   a.cancel = ctx->cancel_dev;
   a.deadlineNs = 0;
-  a.refillMin = 8;
-  if (const char *e = std::getenv("MCB_REFILL_MIN")) a.refillMin = std::max(1, std::min(32, std::atoi(e)));
+  {
+    long long vox = 0;
+    for (const Inst &I : insts) vox = std::max(vox, (long long)I.n[0] * I.n[1] * I.n[2]);
+    const mcb_mc_launch L = launch_params(ctx, size_class(vox, grad, n > 1), grad);
+    a.refillMin = L.refillMin;
+    a.scatterMin = L.scatterMin;
+  }
   const size_t dynSmem = grad ? grad_smem_bytes(insts[0].nM, insts[0].nR, 256) : 0;
   if (grad)
     MCB_CUDA(ctx, cudaFuncSetAttribute(transport_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynSmem));
@@ -1243,6 +1265,104 @@ extern "C" mcb_status mcb_mc_grad(mcb_ctx *ctx, const mcb_mc_model *model, const
   const mcb_mc_model *ms[1] = {model};
   mcb_mc_result *rs[1] = {result};
   return run_models(ctx, 1, ms, rs, objectives, grad);
+}
+
+extern "C" int32_t mcb_mc_size_class(const mcb_mc_model *model, int32_t gradient, int32_t batched) {
+  if (!model) return -1;
+  return size_class((long long)model->nx * model->ny * model->nz, gradient != 0, batched != 0);
+}
+
+namespace mcb {
+// Tuning file: one line per (GPU name, class): "<name>\t<class>\t<refillMin>\t<scatterMin>".
+void tune_file_load(mcb_ctx *ctx) {
+  const char *path = std::getenv("MCB_TUNE_FILE");
+  if (!path || !*path) return;
+  FILE *f = std::fopen(path, "r");
+  if (!f) return;
+  char line[512];
+  while (std::fgets(line, sizeof line, f)) {
+    char *tab = std::strchr(line, '\t');
+    if (!tab) continue;
+    *tab = 0;
+    int cls = 0, r = 0, s = 0;
+    if (ctx->gpuName == line && std::sscanf(tab + 1, "%d %d %d", &cls, &r, &s) == 3 && r >= 1 && r <= 32 && s >= 1 &&
+        s <= 32)
+      ctx->tuned[cls] = mcb_mc_launch{r, s};
+  }
+  std::fclose(f);
+}
+
+void tune_file_store(const mcb_ctx *ctx, int cls, const mcb_mc_launch &L) {
+  const char *path = std::getenv("MCB_TUNE_FILE");
+  if (!path || !*path) return;
+  std::vector<std::string> keep;
+  if (FILE *f = std::fopen(path, "r")) {
+    char line[512];
+    char key[320];
+    std::snprintf(key, sizeof key, "%s\t%d\t", ctx->gpuName.c_str(), cls);
+    while (std::fgets(line, sizeof line, f))
+      if (std::strncmp(line, key, std::strlen(key)) != 0) keep.push_back(line);
+    std::fclose(f);
+  }
+  if (FILE *f = std::fopen(path, "w")) {
+    for (const std::string &l : keep) std::fputs(l.c_str(), f);
+    std::fprintf(f, "%s\t%d\t%d\t%d\n", ctx->gpuName.c_str(), cls, L.refillMin, L.scatterMin);
+    std::fclose(f);
+  }
+}
+}  // namespace mcb
+
+extern "C" mcb_status mcb_mc_autotune(mcb_ctx *ctx, const mcb_mc_model *model, double calibrationPackets, int32_t gradient,
+                                      mcb_mc_launch *chosen, double *table) {
+  using namespace mcb;
+  if (!ctx) return MCB_EINVAL;
+  MCB_TRY(validate(ctx, model));
+  if (!(calibrationPackets >= 1)) return set_error(ctx, MCB_EINVAL, "calibrationPackets must be >= 1");
+  mcb_mc_model m = *model;
+  m.nPhotonsRequested = calibrationPackets;
+  m.requestCollectedPhotons = 0;
+  m.nExamplePaths = 0;
+  mcb_mc_result r;
+  std::memset(&r, 0, sizeof r);
+  mcb_mc_objectives obj;
+  std::memset(&obj, 0, sizeof obj);
+  mcb_mc_grad_result g;
+  std::memset(&g, 0, sizeof g);
+  const int cand[4] = {4, 8, 12, 16};
+  mcb_mc_launch best = launch_params(ctx, -1, gradient != 0);
+  double bestMs = 1e300;
+  int row = 0;
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      ctx->force = mcb_mc_launch{cand[a], cand[b]};
+      double ms = 1e300;
+      for (int rep = 0; rep < 2; rep++) {
+        const mcb_mc_model *ms1[1] = {&m};
+        mcb_mc_result *rs1[1] = {&r};
+        const mcb_status st = gradient ? run_models(ctx, 1, ms1, rs1, &obj, &g) : run_models(ctx, 1, ms1, rs1);
+        if (st != MCB_OK) {
+          ctx->force = mcb_mc_launch{0, 0};
+          return st;
+        }
+        ms = std::min(ms, r.kernelMs);
+      }
+      if (table) {
+        table[3 * row] = cand[a];
+        table[3 * row + 1] = cand[b];
+        table[3 * row + 2] = ms;
+      }
+      row++;
+      if (ms < bestMs) {
+        bestMs = ms;
+        best = ctx->force;
+      }
+    }
+  ctx->force = mcb_mc_launch{0, 0};
+  const int cls = size_class((long long)m.nx * m.ny * m.nz, gradient != 0, false);
+  ctx->tuned[cls] = best;
+  tune_file_store(ctx, cls, best);
+  if (chosen) *chosen = best;
+  return MCB_OK;
 }
 
 extern "C" int64_t mcb_mc_tally_count(const mcb_mc_model *model) {

@@ -27,7 +27,8 @@ EXPORTS = ("mcb_ctx_create", "mcb_ctx_destroy", "mcb_last_error", "mcb_cancel_fl
            "mcb_mc_grad", "mcb_heat_forward_static", "mcb_heat_adjoint", "mcb_probe_atomics",
            "mcb_interface_normals", "mcb_downsample_params",
            "mcb_heat_forward", "mcb_heat_state_create", "mcb_heat_state_step", "mcb_heat_state_read",
-           "mcb_heat_state_destroy", "mcb_last_kernel_ms", "mcb_mc_tally_count", "mcb_mc_normalize")
+           "mcb_heat_state_destroy", "mcb_last_kernel_ms", "mcb_mc_tally_count", "mcb_mc_normalize",
+           "mcb_mc_size_class", "mcb_mc_autotune")
 
 
 class MCBError(RuntimeError):
@@ -77,6 +78,10 @@ def lib():
             L.mcb_mc_tally_count.restype = C.c_int64
             L.mcb_mc_normalize.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.POINTER(C.c_double),
                                            C.POINTER(abi.mcb_mc_result)]
+            L.mcb_mc_size_class.argtypes = [C.POINTER(abi.mcb_mc_model), C.c_int32, C.c_int32]
+            L.mcb_mc_size_class.restype = C.c_int32
+            L.mcb_mc_autotune.argtypes = [C.c_void_p, C.POINTER(abi.mcb_mc_model), C.c_double, C.c_int32,
+                                          C.POINTER(abi.mcb_mc_launch), C.POINTER(C.c_double)]
             L.mcb_last_kernel_ms.argtypes = [C.c_void_p]
             L.mcb_last_kernel_ms.restype = C.c_double
             _lib = L
@@ -110,6 +115,21 @@ def mc_run(mc_in, device=0, example_cap=100000, tallies=False):
     rb = abi.McResultBuffers(mc_in, example_cap if mc_in["nExamplePaths"] else 0, nt)
     _check(lib().mcb_mc_run(ctx, C.byref(mb.model), C.byref(rb.result)), ctx)
     return rb.outputs()
+
+
+def mc_autotune(mc_in, calibration_packets=2e5, gradient=False, device=0):
+    """Tunes the transport kernel's warp-grouping parameters for mc_in's size class on this GPU
+    (mcb_mc_autotune); later runs of the class in this process use the choice. Returns
+    dict(refillMin, scatterMin, sizeClass, table [16 x 3]: refillMin, scatterMin, kernel ms)."""
+    ctx = context(device)
+    mb = abi.McModelBuffers(mc_in)
+    ch = abi.mcb_mc_launch()
+    table = np.zeros(48)
+    _check(lib().mcb_mc_autotune(ctx, C.byref(mb.model), float(calibration_packets), int(bool(gradient)), C.byref(ch),
+                                 table.ctypes.data_as(C.POINTER(C.c_double))), ctx)
+    return {"refillMin": ch.refillMin, "scatterMin": ch.scatterMin,
+            "sizeClass": int(lib().mcb_mc_size_class(C.byref(mb.model), int(bool(gradient)), 0)),
+            "table": table.reshape(16, 3)}
 
 
 def mc_normalize(mc_in, tallies, device=0):

@@ -70,3 +70,13 @@ def test_tally_count_layout(name):
     shapes = abi.result_shapes(mc_in)
     if "NFR" in shapes:
         assert int(np.prod(shapes["NFR"])) == nx * ny * nz * nL
+
+
+def test_size_class():
+    """mcb_mc_size_class (host only): voxels in powers of 4, +16 gradient, +32 batched."""
+    from mcmatlab_b200 import abi, native
+    m = abi.mcb_mc_model()
+    for (nx, ny, nz), want in (((2, 2, 2), 1), ((100, 100, 100), 9), ((256, 256, 256), 12), ((1024, 1024, 1024), 15)):
+        m.nx, m.ny, m.nz = nx, ny, nz
+        assert native.lib().mcb_mc_size_class(C.byref(m), 0, 0) == want
+        assert native.lib().mcb_mc_size_class(C.byref(m), 1, 1) == want + 48
