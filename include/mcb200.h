@@ -286,9 +286,10 @@ MCB_API mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *p, cons
  * a PyTorch caching allocator, has already reserved; other streams' work that cudaFree's
  * device-wide synchronisation would stall). Same arguments, outputs and errors as
  * mcb_heat_forward. Its working set lives in one static 32 MiB device array of the library:
- * 66 bytes per voxel (58 without damage, 62 with damage but no light) plus 8 per sensor and
- * step (sensorTemps history) and small per-medium tables; larger problems return MCB_EINVAL
- * naming the limit. The context comes from mcb_ctx_create, which does allocate: create it
+ * 26 bytes per voxel (18 without damage, 22 with damage but no light; the per-voxel grids are
+ * stored with nx rounded up to a multiple of 16), about a 107^3 grid, or 66 bytes per voxel for
+ * grids with an axis longer than 512; plus 8 per sensor and step (sensorTemps history) and
+ * small per-medium tables. Larger problems return MCB_EINVAL naming the limit. The context comes from mcb_ctx_create, which does allocate: create it
  * at set-up. The first call on a device performs set-up (cudaGetSymbolAddress of the scratch).
  * The call is synchronous (it waits for ctx's stream and reads its events before returning), so
  * it must not be made while ctx's stream is being captured. There is one scratch per device:
