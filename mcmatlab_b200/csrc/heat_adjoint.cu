@@ -232,95 +232,218 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
   }
 }
 
-// lambda^n, dJ/dQ and dJ/dc of one reversed step (7-point stencil over every voxel).
-// bounded for 3 blocks of 512 threads per SM: 40 registers with a few spills, which lets more
-// row blocks share an SM and measured 3% faster reverse sweeps than 57 registers without spills
-__global__ void __launch_bounds__(512, 3) adj_assemble_kernel(AdjDev a) {
+
+// Running per-voxel maximum over the peak list after forward step `step`.
+// The assembly marching along z: a block owns a 32 x 8 tile of (x, y) columns, one thread per
+// column, and walks the planes iz = 0 .. nz-1. Arrays read with in-plane neighbours are staged in
+// shared memory per plane with a one-voxel halo (r1, T^n and the media on a ring of three planes,
+// which also serves their z neighbours; A1 with its x halo and r2, A2 with their y halos on two
+// planes), r3 and T^{n+1} (z neighbours only) on a ring of three centre tiles. Each array is read
+// from memory once (plus the tile halos) instead of once per neighbour, and the loads of the
+// plane after next are in flight while a plane is assembled. Same arithmetic as
+// adj_assemble_kernel, voxel by voxel.
+constexpr int kZX = 32, kZY = 8, kZHX = kZX + 2, kZHY = kZY + 2;
+constexpr int kZHN = kZHX * kZHY;  // halo tile (340)
+constexpr int kZCN = kZX * kZY;    // centre tile (256)
+constexpr int kZA1 = kZY * kZHX;   // x-halo tile (272)
+constexpr int kZR2 = kZHY * kZX;   // y-halo tile (320)
+constexpr int kZChunk = 25;        // planes per block
+
+__global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   const HeatDev &h = a.h;
   __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
+  __shared__ float sR1[3][kZHN], sTN[3][kZHN], sR3[3][kZCN], sTP[3][kZCN];
+  __shared__ float sA1[2][kZA1], sR2[2][kZR2], sA2[2][kZR2];
+  __shared__ uint8_t sM[3][kZHN + 4];
   const int nM = h.nM, nM2 = nM * nM;
   for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) sdc[k] = 0.0;
-  __syncthreads();
-  const long long sxy = (long long)h.nx * h.ny;
-  const float dt = h.dt, hdt = h.hdt;
-  // same-medium faces (the common case) accumulate in registers, flushed when the medium changes
-  int curM = -1;
-  float same[3] = {0.f, 0.f, 0.f};
-  const int rows = h.ny * h.nz;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x)
-  for (int ix = threadIdx.x; ix < h.nx; ix += blockDim.x) {
-    const int iy = row % h.ny, iz = row / h.ny;
-    const long long v = ix + (long long)row * h.nx;
-    const int mv = h.M[v];
-    const bool nsv = !sinked(h, ix, iy, iz);
-    const float r1v = a.r1[v], r2v = a.r2[v], r3v = a.r3[v];
-    const float tv = a.Tn[v];
-    if (nsv && mv != curM) {
-      if (curM >= 0)
-        for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
-      curM = mv;
-      same[0] = same[1] = same[2] = 0.f;
-    }
-    float lam = r1v;
-    // interior of a homogeneous region with no heat-sinked neighbour: all six faces share one
-    // coefficient per direction, every load is independent of the others
-    const bool interior = h.nb[v] == 0 && !(h.hs && (ix <= 1 || ix >= h.nx - 2 || iy <= 1 || iy >= h.ny - 2 ||
-                                                     iz <= 1 || iz >= h.nz - 2));
-    if (interior) {
-      const long long sy = h.nx, sz = sxy;
-      const float cx = cf(h, mv, mv, 0), cy = cf(h, mv, mv, 1), cz = cf(h, mv, mv, 2);
-      const float r1xl = a.r1[v - 1], r1xr = a.r1[v + 1], r1yl = a.r1[v - sy], r1yr = a.r1[v + sy];
-      const float r1zl = a.r1[v - sz], r1zr = a.r1[v + sz];
-      const float r2yl = a.r2[v - sy], r2yr = a.r2[v + sy], r3zl = a.r3[v - sz], r3zr = a.r3[v + sz];
-      const float txl = a.Tn[v - 1], txr = a.Tn[v + 1], tyl = a.Tn[v - sy], tyr = a.Tn[v + sy];
-      const float tzl = a.Tn[v - sz], tzr = a.Tn[v + sz];
-      const float a1v = a.A1[v], a1l = a.A1[v - 1], a1r = a.A1[v + 1];
-      const float a2v = a.A2[v], a2l = a.A2[v - sy], a2r = a.A2[v + sy];
-      const float tpv = a.Tp[v], tpl = a.Tp[v - sz], tpr = a.Tp[v + sz];
-      const float qy = dt * r1v - hdt * r2v, qz = dt * r1v - hdt * r3v;
-      lam += cx * hdt * (r1xl + r1xr - 2.f * r1v) +
-             cy * ((dt * r1yl - hdt * r2yl) + (dt * r1yr - hdt * r2yr) - 2.f * qy) +
-             cz * ((dt * r1zl - hdt * r3zl) + (dt * r1zr - hdt * r3zr) - 2.f * qz);
-      same[0] += hdt * r1v * ((txl + a1l) + (txr + a1r) - 2.f * (tv + a1v));
-      same[1] += dt * r1v * (tyl + tyr - 2.f * tv) + hdt * r2v * ((a2l - tyl) + (a2r - tyr) - 2.f * (a2v - tv));
-      same[2] += dt * r1v * (tzl + tzr - 2.f * tv) + hdt * r3v * ((tpl - tzl) + (tpr - tzr) - 2.f * (tpv - tv));
-      a.lamOut[v] = lam;
-      if (a.dQ) a.dQ[v] += dt * r1v;
-      continue;
-    }
+  const int nx = h.nx, ny = h.ny, nz = h.nz;
+  const long long sxy = (long long)nx * ny;
+  const int x0 = blockIdx.x * kZX, y0 = blockIdx.y * kZY;
+  const int t = threadIdx.x, tx = t % kZX, ty = t / kZX;
+  // this thread's staging slots: halo elements t and t + 256 (< 340), centre element t, x-halo
+  // elements t and t + 256 (< 272), y-halo elements t and t + 256 (< 320)
+  auto hoff = [&](int e, int &x, int &y) { x = x0 - 1 + e % kZHX; y = y0 - 1 + e / kZHX; };
+  auto inside = [&](int x, int y) { return x >= 0 && x < nx && y >= 0 && y < ny; };
+  // prefetch registers of one plane
+  float pR1[2], pTN[2], pR3, pTP, pA1[2], pR2[2], pA2[2];
+  int pM[2];
+  auto load_ring = [&](int iz) {
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const int pos = d == 0 ? ix : (d == 1 ? iy : iz);
-      const int n = d == 0 ? h.nx : (d == 1 ? h.ny : h.nz);
-      const long long st = d == 0 ? 1 : (d == 1 ? h.nx : sxy);
-      const float qv = d == 0 ? hdt * r1v : (d == 1 ? dt * r1v - hdt * r2v : dt * r1v - hdt * r3v);
-      // the field whose face differences carry dJ/dc along d, and its weight at v
-      const float pv = d == 0 ? tv + a.A1[v] : (d == 1 ? a.A2[v] - tv : a.Tp[v] - tv);
-#pragma unroll
-      for (int side = -1; side <= 1; side += 2) {
-        if ((side < 0 && pos == 0) || (side > 0 && pos == n - 1)) continue;
-        const long long u = v + side * st;
-        const int mu = h.M[u];
-        const int ux = d == 0 ? ix + side : ix, uy = d == 1 ? iy + side : iy, uz = d == 2 ? iz + side : iz;
-        if (!sinked(h, ux, uy, uz)) {
-          const float r1u = a.r1[u];
-          const float qu = d == 0 ? hdt * r1u : (d == 1 ? dt * r1u - hdt * a.r2[u] : dt * r1u - hdt * a.r3[u]);
-          lam += cf(h, mu, mv, d) * qu;
-        }
-        if (nsv) {
-          lam -= cf(h, mv, mu, d) * qv;
-          const float tu = a.Tn[u];
-          float contrib;
-          if (d == 0) contrib = hdt * r1v * ((tu + a.A1[u]) - pv);
-          else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((a.A2[u] - tu) - pv);
-          else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((a.Tp[u] - tu) - pv);
-          if (mu == mv) same[d] += contrib;
-          else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      pR1[q] = pTN[q] = 0.f;
+      pM[q] = 0;
+      if (e < kZHN) {
+        int x, y;
+        hoff(e, x, y);
+        if (inside(x, y)) {
+          const long long v = x + (long long)y * nx + iz * sxy;
+          pR1[q] = a.r1[v];
+          pTN[q] = a.Tn[v];
+          pM[q] = h.M[v];
         }
       }
     }
-    a.lamOut[v] = lam;
-    if (a.dQ && nsv) a.dQ[v] += dt * r1v;
+    pR3 = pTP = 0.f;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x < nx && y < ny) {
+      const long long v = x + (long long)y * nx + iz * sxy;
+      pR3 = a.r3[v];
+      pTP = a.Tp[v];
+    }
+  };
+  auto store_ring = [&](int slot) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      if (e < kZHN) {
+        sR1[slot][e] = pR1[q];
+        sTN[slot][e] = pTN[q];
+        sM[slot][e] = (uint8_t)pM[q];
+      }
+    }
+    sR3[slot][t] = pR3;
+    sTP[slot][t] = pTP;
+  };
+  auto load_single = [&](int iz) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      pA1[q] = pR2[q] = pA2[q] = 0.f;
+      if (e < kZA1) {
+        const int x = x0 - 1 + e % kZHX, y = y0 + e / kZHX;
+        if (inside(x, y)) pA1[q] = a.A1[x + (long long)y * nx + iz * sxy];
+      }
+      if (e < kZR2) {
+        const int x = x0 + e % kZX, y = y0 - 1 + e / kZX;
+        if (inside(x, y)) {
+          const long long v = x + (long long)y * nx + iz * sxy;
+          pR2[q] = a.r2[v];
+          pA2[q] = a.A2[v];
+        }
+      }
+    }
+  };
+  auto store_single = [&](int slot) {
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      if (e < kZA1) sA1[slot][e] = pA1[q];
+      if (e < kZR2) {
+        sR2[slot][e] = pR2[q];
+        sA2[slot][e] = pA2[q];
+      }
+    }
+  };
+  // this block's planes [z0, z1) (blockIdx.z: z chunks of kZChunk planes, for more blocks in flight)
+  const int z0 = blockIdx.z * kZChunk, z1 = min(nz, z0 + kZChunk);
+  // prologue: planes z0 - 1, z0, z0 + 1 of the rings and plane z0 of the single-plane tiles
+  // staged, plane z0 + 2 of the rings and z0 + 1 of the others in flight
+  if (z0 > 0) {
+    load_ring(z0 - 1);
+    store_ring((z0 - 1) % 3);
+  }
+  load_ring(z0);
+  store_ring(z0 % 3);
+  if (z0 + 1 < nz) {
+    load_ring(z0 + 1);
+    store_ring((z0 + 1) % 3);
+  }
+  load_single(z0);
+  store_single(z0 & 1);
+  if (z0 + 2 < nz && z0 + 2 <= z1) load_ring(z0 + 2);
+  if (z0 + 1 < z1) load_single(z0 + 1);
+  const float dt = h.dt, hdt = h.hdt;
+  int curM = -1;
+  float same[3] = {0.f, 0.f, 0.f};
+  const int ix = x0 + tx, iy = y0 + ty;
+  const bool col = ix < nx && iy < ny;
+  const int hc = (ty + 1) * kZHX + tx + 1;  // centre in the halo tile
+  for (int iz = z0; iz < z1; iz++) {
+    __syncthreads();
+    const int sc = iz % 3, sp = (iz + 1) % 3, sm = (iz + 2) % 3, q1 = iz & 1;
+    if (col) {
+      const long long v = ix + (long long)iy * nx + iz * sxy;
+      const int mv = sM[sc][hc];
+      const bool nsv = !sinked(h, ix, iy, iz);
+      const float r1v = sR1[sc][hc], r2v = sR2[q1][(ty + 1) * kZX + tx], r3v = sR3[sc][t];
+      const float tv = sTN[sc][hc];
+      const float a1v = sA1[q1][ty * kZHX + tx + 1], a2v = sA2[q1][(ty + 1) * kZX + tx], tpv = sTP[sc][t];
+      if (nsv && mv != curM) {
+        if (curM >= 0)
+          for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
+        curM = mv;
+        same[0] = same[1] = same[2] = 0.f;
+      }
+      float lam = r1v;
+      const bool interior = h.nb[v] == 0 && !(h.hs && (ix <= 1 || ix >= nx - 2 || iy <= 1 || iy >= ny - 2 ||
+                                                       iz <= 1 || iz >= nz - 2));
+      if (interior) {
+        const float cx = cf(h, mv, mv, 0), cy = cf(h, mv, mv, 1), cz = cf(h, mv, mv, 2);
+        const float r1xl = sR1[sc][hc - 1], r1xr = sR1[sc][hc + 1], r1yl = sR1[sc][hc - kZHX],
+                    r1yr = sR1[sc][hc + kZHX];
+        const float r1zl = sR1[sm][hc], r1zr = sR1[sp][hc];
+        const float r2yl = sR2[q1][ty * kZX + tx], r2yr = sR2[q1][(ty + 2) * kZX + tx];
+        const float r3zl = sR3[sm][t], r3zr = sR3[sp][t];
+        const float txl = sTN[sc][hc - 1], txr = sTN[sc][hc + 1], tyl = sTN[sc][hc - kZHX], tyr = sTN[sc][hc + kZHX];
+        const float tzl = sTN[sm][hc], tzr = sTN[sp][hc];
+        const float a1l = sA1[q1][ty * kZHX + tx], a1r = sA1[q1][ty * kZHX + tx + 2];
+        const float a2l = sA2[q1][ty * kZX + tx], a2r = sA2[q1][(ty + 2) * kZX + tx];
+        const float tpl = sTP[sm][t], tpr = sTP[sp][t];
+        const float qy = dt * r1v - hdt * r2v, qz = dt * r1v - hdt * r3v;
+        lam += cx * hdt * (r1xl + r1xr - 2.f * r1v) +
+               cy * ((dt * r1yl - hdt * r2yl) + (dt * r1yr - hdt * r2yr) - 2.f * qy) +
+               cz * ((dt * r1zl - hdt * r3zl) + (dt * r1zr - hdt * r3zr) - 2.f * qz);
+        same[0] += hdt * r1v * ((txl + a1l) + (txr + a1r) - 2.f * (tv + a1v));
+        same[1] += dt * r1v * (tyl + tyr - 2.f * tv) + hdt * r2v * ((a2l - tyl) + (a2r - tyr) - 2.f * (a2v - tv));
+        same[2] += dt * r1v * (tzl + tzr - 2.f * tv) + hdt * r3v * ((tpl - tzl) + (tpr - tzr) - 2.f * (tpv - tv));
+        a.lamOut[v] = lam;
+        if (a.dQ) a.dQ[v] += dt * r1v;
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const int pos = d == 0 ? ix : (d == 1 ? iy : iz);
+          const int n = d == 0 ? nx : (d == 1 ? ny : nz);
+          const float qv = d == 0 ? hdt * r1v : (d == 1 ? dt * r1v - hdt * r2v : dt * r1v - hdt * r3v);
+          const float pv = d == 0 ? tv + a1v : (d == 1 ? a2v - tv : tpv - tv);
+#pragma unroll
+          for (int side = -1; side <= 1; side += 2) {
+            if ((side < 0 && pos == 0) || (side > 0 && pos == n - 1)) continue;
+            // the neighbour u in the staged tiles
+            const int hu = d == 0 ? hc + side : (d == 1 ? hc + side * kZHX : hc);
+            const int rs = d == 2 ? (side < 0 ? sm : sp) : sc;
+            const int mu = sM[rs][hu];
+            const float r1u = sR1[rs][hu], tu = sTN[rs][hu];
+            const int ux = d == 0 ? ix + side : ix, uy = d == 1 ? iy + side : iy, uz = d == 2 ? iz + side : iz;
+            if (!sinked(h, ux, uy, uz)) {
+              const float qu = d == 0   ? hdt * r1u
+                               : d == 1 ? dt * r1u - hdt * sR2[q1][(ty + 1 + side) * kZX + tx]
+                                        : dt * r1u - hdt * sR3[rs][t];
+              lam += cf(h, mu, mv, d) * qu;
+            }
+            if (nsv) {
+              lam -= cf(h, mv, mu, d) * qv;
+              float contrib;
+              if (d == 0) contrib = hdt * r1v * ((tu + sA1[q1][ty * kZHX + tx + 1 + side]) - pv);
+              else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((sA2[q1][(ty + 1 + side) * kZX + tx] - tu) - pv);
+              else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((sTP[rs][t] - tu) - pv);
+              if (mu == mv) same[d] += contrib;
+              else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
+            }
+          }
+        }
+        a.lamOut[v] = lam;
+        if (a.dQ && nsv) a.dQ[v] += dt * r1v;
+      }
+    }
+    __syncthreads();
+    // stage the prefetched planes (ring: iz + 2 into the slot of iz - 1; single tiles: iz + 1)
+    // and start the loads of the next ones
+    if (iz + 2 < nz && iz + 2 <= z1) store_ring(sm);
+    if (iz + 1 < z1) store_single((iz + 1) & 1);
+    if (iz + 3 < nz && iz + 3 <= z1) load_ring(iz + 3);
+    if (iz + 2 < z1) load_single(iz + 2);
   }
   if (curM >= 0)
     for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
@@ -329,7 +452,6 @@ __global__ void __launch_bounds__(512, 3) adj_assemble_kernel(AdjDev a) {
     if (sdc[k] != 0.0) atomicAdd(&a.dc[k], sdc[k]);
 }
 
-// Running per-voxel maximum over the peak list after forward step `step`.
 __global__ void peak_track_kernel(const float *T, int nP, const int *idx, float *val, int *at, int step) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nP; k += gridDim.x * blockDim.x) {
     const float t = T[idx[k]];
@@ -498,6 +620,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   // one thread per x position of a row (a warp multiple, at most 512): no idle second pass
   const int rowThreads = std::min(512, (nx + 31) / 32 * 32);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
+  const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
 
   // forward sweep: checkpoints every K steps, running maxima of the peak list
   ADJ_CUDA(cudaEventRecord(ctx->ev0, st));
@@ -539,7 +662,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       else if (tw == 16) adj_launch_yz<16>(a, false, gridYZ, st);
       else adj_launch_yz<8>(a, false, gridYZ, st);
       adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
-      adj_assemble_kernel<<<gridE, rowThreads, 0, st>>>(a);
+      adj_assemble_z_kernel<<<gridZ, 256, 0, st>>>(a);
       if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
       std::swap(lam, lamNext);
     }

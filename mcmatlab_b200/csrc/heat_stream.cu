@@ -662,6 +662,7 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = align1024(smem_raw);
   __shared__ unsigned int mloc[256];
+  __shared__ float2 sdmg[256];  // Arrhenius exponent terms per medium (y = 0: no damage)
   __shared__ float hd[256];   // H(m, m) of this direction
   __shared__ float hsv[256];  // 1 / b*(m) of this direction
   const int n = ZP ? h.nz : h.ny;
@@ -686,7 +687,10 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
     hd[k] = Hl[k * nM + k];
     const float4 f4 = h.Hs[k];
     hsv[k] = ZP ? f4.z : f4.y;
-    if (ZP) mloc[k] = 0u;
+    if (ZP) {
+      mloc[k] = 0u;
+      sdmg[k] = h.dOmega ? h.dmg[k] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   auto issue = [&](int tile, int stg) {
@@ -713,17 +717,6 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
   }
   int curM = -1;
   float curMax = 0.f;  // running maximum of the deviation in medium curM
-  // warp-collective flush of the lanes in `lanes` (all lanes of the warp call it): lanes flushing
-  // the same medium combine their maxima first, so each medium takes one shared atomic per warp
-  auto flush_max = [&](bool flush) {
-    const unsigned want = __ballot_sync(0xffffffffu, flush && curM >= 0);
-    if (!want) return;
-    if (flush && curM >= 0) {
-      const unsigned peers = __match_any_sync(want, curM);
-      const unsigned enc = __reduce_max_sync(peers, enc_max((float)((double)curMax + h.base)));
-      if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(&mloc[curM], enc);
-    }
-  };
   int it = 0;
   for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
     const int stg = it & 1;
@@ -872,8 +865,8 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
         if (ZP) {
           const float tnew = r[k];
           const int m = med(s + k);  // the stage still holds this tile (reissued below)
-          if (h.dOmega) {
-            const float2 dg = h.dmg[m];
+          {
+            const float2 dg = sdmg[m];
             if (dg.y > 0.f) {
               // Arrhenius integral with the mid-step temperature (finiteElementHeatPropagator.c:600-602):
               // log A - E / (R (T0 + d)) = x0 + (E/R) d / (T0 (T0 + d)), x0 formed in FP64 per call
@@ -886,18 +879,15 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
           h.A[v] = r[k];
         }
       }
-      if (ZP) {
-        // running maxima: a lane whose medium changes flushes (warp-collectively, every lane calls)
-        const int mk = k < nv ? med(s + k) : curM;
-        const bool change = mk != curM;
-        flush_max(change);
-        if (k < nv) {
-          if (change) {
-            curM = mk;
-            curMax = r[k];
-          } else {
-            curMax = fmaxf(curMax, r[k]);
-          }
+      if (ZP && k < nv) {
+        // running maxima per lane, flushed to shared memory when the lane's medium changes
+        const int mk = med(s + k);
+        if (mk != curM) {
+          if (curM >= 0) atomicMax(&mloc[curM], enc_max((float)((double)curMax + h.base)));
+          curM = mk;
+          curMax = r[k];
+        } else {
+          curMax = fmaxf(curMax, r[k]);
         }
       }
     }
@@ -914,7 +904,7 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
     }
   }
   if (ZP) {
-    flush_max(true);
+    if (curM >= 0) atomicMax(&mloc[curM], enc_max((float)((double)curMax + h.base)));
     __syncthreads();
     for (int k = threadIdx.x; k < nM; k += blockDim.x)
       if (mloc[k]) atomicMax(&h.maxEnc[k], mloc[k]);
