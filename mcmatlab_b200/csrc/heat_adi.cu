@@ -1019,3 +1019,13 @@ extern "C" mcb_status mcb_heat_forward_static(mcb_ctx *ctx, const mcb_heat_param
   ctx->lastKernelMs = ms;
   return MCB_OK;
 }
+
+namespace mcb {
+mcb_status stream_state_create(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T) {
+  s->ctx = ctx;
+  MCB_TRY(stream_alloc(ctx, s, p, false));
+  MCB_TRY(stream_upload(ctx, s, p, T, nullptr));
+  if (p->lightsOn) MCB_TRY(stream_upload_q(ctx, s, p->dTdt_abs));
+  return MCB_OK;
+}
+}  // namespace mcb

@@ -534,7 +534,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   const size_t grid4 = 4 * (size_t)L;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t bytes = al(grid4) * (size_t)(nSeg + K + 1 + 9) + al(8 * (size_t)nM * nM * 3) + al(16) +
-                       al(12 * (size_t)std::max(nD, 1)) + al(12 * (size_t)std::max(nP, 1)) + al(4 * (size_t)std::max(nP, 1)) +
+                       al(12 * (size_t)std::max(nD, 1)) + al(12 * (size_t)std::max(nP, 1)) + al(8 * (size_t)std::max(nP, 1)) +
                        4096;
   void *block = nullptr;
   rc = pool_get(ctx, SLOT_HEAT_ADJ, bytes, &block);
@@ -569,7 +569,13 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   float *pWD = (float *)take(4 * (size_t)std::max(nP, 1));
   float *pVal = (float *)take(4 * (size_t)std::max(nP, 1));
   int *pStepD = (int *)take(4 * (size_t)std::max(nP, 1));
+  mcb_heat_state ss;  // streamed state of the forward sweeps (below)
+  StreamStepper *sk = nullptr;
   auto fail = [&](mcb_status r) {
+    if (sk) {
+      stream_stepper_free(sk);
+      heat_state_release(&ss);
+    }
     heat_state_release(&s);
     return r;
   };
@@ -622,12 +628,41 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
   const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
 
+  // The forward sweeps (checkpoints, segment recomputation) step a streamed state where the grid
+  // allows: the same steps up to FP32 rounding at the streamed stepper's speed. The reverse
+  // sweep keeps the factored state's LU pivots for its transposed solves.
+  int *pIdxS = pIdxD;
+  if (stream_supported(p.nx, p.ny, p.nz)) {
+    rc = stream_state_create(ctx, &ss, &p, T0);
+    if (rc == MCB_OK) rc = stream_stepper_new(ctx, &ss, &p, &sk);
+    if (rc != MCB_OK) {
+      if (sk) stream_stepper_free(sk);
+      sk = nullptr;
+      heat_state_release(&ss);
+      return fail(rc);
+    }
+    if (nP) {
+      // the peak list's voxels in the streamed state's pitched grid
+      std::vector<int> pIdxP(nP);
+      for (int k = 0; k < nP; k++) pIdxP[k] = (int)stream_pitched_index(&ss, pIdx[k]);
+      pIdxS = (int *)take(4 * (size_t)nP);
+      ADJ_CUDA(cudaMemcpyAsync(pIdxS, pIdxP.data(), 4 * (size_t)nP, cudaMemcpyHostToDevice, st));
+      ADJ_CUDA(cudaStreamSynchronize(st));
+    }
+  }
   // forward sweep: checkpoints every K steps, running maxima of the peak list
   ADJ_CUDA(cudaEventRecord(ctx->ev0, st));
   for (long long n = 0; n < nt; n++) {
-    if (n % K == 0) ADJ_CUDA(cudaMemcpyAsync(ckpt + (size_t)(n / K) * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
-    heat_step_launch(ks, st);
-    if (nP) peak_track_kernel<<<gridL, 256, 0, st>>>(s.T, nP, pIdxD, pVal, pStepD, (int)(n + 1));
+    float *ck = ckpt + (size_t)(n / K) * L;
+    if (sk) {
+      if (n % K == 0) stream_dense_copy(ctx, &ss, ck, st);
+      stream_stepper_launch(sk, st);
+      if (nP) peak_track_kernel<<<gridL, 256, 0, st>>>(ss.T, nP, pIdxS, pVal, pStepD, (int)(n + 1));
+    } else {
+      if (n % K == 0) ADJ_CUDA(cudaMemcpyAsync(ck, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+      heat_step_launch(ks, st);
+      if (nP) peak_track_kernel<<<gridL, 256, 0, st>>>(s.T, nP, pIdxD, pVal, pStepD, (int)(n + 1));
+    }
   }
   ADJ_CUDA(cudaGetLastError());
   ADJ_CUDA(cudaEventRecord(ctx->ev1, st));
@@ -641,10 +676,18 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   for (long long seg = nSeg - 1; seg >= 0; seg--) {
     const long long n0 = seg * K, n1 = std::min(n0 + K, nt);
     ADJ_CUDA(cudaMemcpyAsync(ring, ckpt + (size_t)seg * L, grid4, cudaMemcpyDeviceToDevice, st));
-    ADJ_CUDA(cudaMemcpyAsync(s.T, ring, grid4, cudaMemcpyDeviceToDevice, st));
-    for (long long j = 1; j <= n1 - n0; j++) {
-      heat_step_launch(ks, st);
-      ADJ_CUDA(cudaMemcpyAsync(ring + (size_t)j * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+    if (sk) {
+      stream_dense_set(ctx, &ss, ring, st);
+      for (long long j = 1; j <= n1 - n0; j++) {
+        stream_stepper_launch(sk, st);
+        stream_dense_copy(ctx, &ss, ring + (size_t)j * L, st);
+      }
+    } else {
+      ADJ_CUDA(cudaMemcpyAsync(s.T, ring, grid4, cudaMemcpyDeviceToDevice, st));
+      for (long long j = 1; j <= n1 - n0; j++) {
+        heat_step_launch(ks, st);
+        ADJ_CUDA(cudaMemcpyAsync(ring + (size_t)j * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+      }
     }
     for (long long n = n1 - 1; n >= n0; n--) {
       a.Tn = ring + (size_t)(n - n0) * L;
@@ -689,6 +732,10 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   out->forwardMs = msF;
   out->adjointMs = msR;
   ctx->lastKernelMs = msF + msR;
+  if (sk) {
+    stream_stepper_free(sk);
+    heat_state_release(&ss);
+  }
   heat_state_release(&s);
   return MCB_OK;
 }

@@ -84,7 +84,16 @@ void heat_step_launch(const HeatStepper &k, cudaStream_t st);
 void heat_damage_table(const mcb_heat_params *p, double base, float2 *out);
 
 // Streamed stepper (heat_stream.cu).
+struct StreamStepper;  // launch configuration of one streamed step (heat_stream.cu)
 bool stream_supported(int nx, int ny, int nz);
+// A streamed state for p's grid holding T (no damage), with p's source when the light is on
+// (heat_adi.cu); release with heat_state_release.
+mcb_status stream_state_create(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, const float *T);
+// Creates *out (the set-up of stream_step) for stepping s one step at a time (no sensors);
+// release with stream_stepper_free.
+mcb_status stream_stepper_new(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, StreamStepper **out);
+void stream_stepper_free(StreamStepper *k);
+void stream_stepper_launch(const StreamStepper *k, cudaStream_t st);
 StreamShape stream_shape(int nx, int ny, int nz);
 int stream_warmup(const float *c, float hdt, int nM);
 void stream_carve(const std::function<void *(size_t)> &take, mcb_heat_state *s, const mcb_heat_params *p, bool damage,
@@ -95,5 +104,11 @@ mcb_status stream_upload_q(mcb_ctx *ctx, mcb_heat_state *s, const float *Q);
 mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, double *sensorTemps,
                        float *maxMediaTemps, bool graphs);
 mcb_status stream_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Omega);
+// T of a streamed state (pitched deviations) into a dense array of deviations, and back;
+// asynchronous.
+void stream_dense_copy(mcb_ctx *ctx, const mcb_heat_state *s, float *dense, cudaStream_t st);
+void stream_dense_set(mcb_ctx *ctx, mcb_heat_state *s, const float *dense, cudaStream_t st);
+// Index of voxel v (dense, column-major) in a streamed state's pitched grids.
+long long stream_pitched_index(const mcb_heat_state *s, long long v);
 
 }  // namespace mcb

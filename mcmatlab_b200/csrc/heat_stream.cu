@@ -1275,22 +1275,31 @@ mcb_status stream_upload_q(mcb_ctx *ctx, mcb_heat_state *s, const float *Q) {
   return MCB_OK;
 }
 
-// Runs p->steps steps on the device-resident streamed state. Sensor and maximum outputs go to
-// host memory; `sens` is the device buffer of the sensor history ([nS x (steps + 1)] doubles).
-mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, double *sensorTemps,
-                       float *maxMediaTemps, bool graphs) {
+// Launch configuration of one streamed step on a state.
+struct StreamStepper {
+  StreamDev h;
+  StreamShape S;
+  const StreamMaps *maps = nullptr;
+  int K = 8, XG = 16, gX = 1, gY = 1, gZ = 1;
+  size_t xs = 0;
+  bool colY = true, colZ = true;
+};
+
+// Per-call set-up of the streamed stepper on a state: the per-call tables (H = dt/2 c in FP32, as
+// the stepper multiplies them, and its diagonal and fixed points, formed on the device; the
+// damage exponents about the base temperature; the pivot warm-up length), cleared maxima, step
+// counter and damage increments, kernel attributes and grids. `sens` is the device buffer of the
+// sensor history ([nS x (steps + 1)] doubles) or nullptr.
+mcb_status stream_setup(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, StreamStepper *out) {
   cudaStream_t st = ctx->stream;
   const StreamShape &S = s->shape;
-  const long long L = (long long)S.nx * S.ny * S.nz, nt = p->steps;
+  const long long L = (long long)S.nx * S.ny * S.nz;
   const int nM = p->nM, nS = p->nSensors;
   if (p->lightsOn && !s->qValid) return set_error(ctx, MCB_EINVAL, "dTdt_abs missing while lightsOn");
   if (s->codeHs != (int)(p->heatBoundaryType != 0)) {
     code_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->M, s->code, Pitch{S.nx, S.ny, S.nz, S.px}, p->heatBoundaryType != 0, L);
     s->codeHs = (int)(p->heatBoundaryType != 0);
   }
-  // per-call tables (no host allocation): H = dt/2 c in FP32, as the stepper multiplies them, and
-  // its diagonal, formed on the device; the damage exponents about the base temperature; and the
-  // pivot warm-up length
   const float hdt = (float)(p->dt / 2);
   MCB_CUDA(ctx, cudaMemcpyAsync(s->H, p->dTdtperdeltaT, 12 * (size_t)nM * nM, cudaMemcpyHostToDevice, st));
   h_table_kernel<<<std::max(1, std::min(1024, (3 * nM * nM + 255) / 256)), 256, 0, st>>>(s->H, s->Hd, hdt, nM);
@@ -1302,7 +1311,9 @@ mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   MCB_CUDA(ctx, cudaMemsetAsync(s->step, 0, 16, st));
   if (s->dOm) MCB_CUDA(ctx, cudaMemsetAsync(s->dOm, 0, 4 * (size_t)S.Lp, st));
 
-  StreamDev h{};
+  StreamStepper &k = *out;
+  StreamDev &h = k.h;
+  h = StreamDev{};
   h.nx = S.nx; h.ny = S.ny; h.nz = S.nz; h.nM = nM; h.px = S.px; h.W = std::min(W, std::max({S.nx, S.ny, S.nz}));
   h.sxy = (long long)S.px * S.ny;
   h.T = s->T; h.A = s->A; h.M = s->M; h.code = s->code;
@@ -1313,36 +1324,94 @@ mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p
   h.nS = nS; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = sens; h.stepCounter = s->step; h.err = s->step + 1;
   s->lastW = h.W;
 
-  const int K = x_chunk(S.nx), XG = x_lanes(S.nx), XL = x_tile_lines(S.nx);
-  const size_t xs = x_smem(S.px, h.Q != nullptr, S.nx);
-  if (XG == 16) MCB_TRY((x_attr<8, 16>(ctx, xs)));
-  else if (K == 8) MCB_TRY((x_attr<8, 32>(ctx, xs)));
-  else if (K == 12) MCB_TRY((x_attr<12, 32>(ctx, xs)));
-  else MCB_TRY((x_attr<16, 32>(ctx, xs)));
+  k.S = S;
+  k.maps = s->maps;
+  k.K = x_chunk(S.nx);
+  k.XG = x_lanes(S.nx);
+  const int XL = x_tile_lines(S.nx);
+  k.xs = x_smem(S.px, h.Q != nullptr, S.nx);
+  if (k.XG == 16) MCB_TRY((x_attr<8, 16>(ctx, k.xs)));
+  else if (k.K == 8) MCB_TRY((x_attr<8, 32>(ctx, k.xs)));
+  else if (k.K == 12) MCB_TRY((x_attr<12, 32>(ctx, k.xs)));
+  else MCB_TRY((x_attr<16, 32>(ctx, k.xs)));
   int bpsY = 1, bpsZ = 1;
-  const bool colY = S.ny <= kColMaxN, colZ = S.nz <= kColMaxN;
-  if (colY) MCB_TRY(col_occupancy<false>(ctx, S.ny, &bpsY));
+  k.colY = S.ny <= kColMaxN;
+  k.colZ = S.nz <= kColMaxN;
+  if (k.colY) MCB_TRY(col_occupancy<false>(ctx, S.ny, &bpsY));
   else MCB_TRY(yz_setup<false>(ctx, S.ny, &bpsY));
-  if (colZ) MCB_TRY(col_occupancy<true>(ctx, S.nz, &bpsZ));
+  if (k.colZ) MCB_TRY(col_occupancy<true>(ctx, S.nz, &bpsZ));
   else MCB_TRY(yz_setup<true>(ctx, S.nz, &bpsZ));
-  const int xbps = std::max(1, std::min(XG == 16 ? 3 : 2, (int)((227u * 1024u) / (unsigned)(xs + 1024))));
+  const int xbps = std::max(1, std::min(k.XG == 16 ? 3 : 2, (int)((227u * 1024u) / (unsigned)(k.xs + 1024))));
   const long long tilesX = (long long)((S.ny + XL - 1) / XL) * S.nz;
-  const long long tilesY = (long long)((S.nx + (colY ? 31 : kTW - 1)) / (colY ? 32 : kTW)) * S.nz;
-  const long long tilesZ = (long long)((S.nx + (colZ ? 31 : kTW - 1)) / (colZ ? 32 : kTW)) * S.ny;
-  const int gX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * xbps);
-  const int gY = (int)std::min<long long>(tilesY, (long long)ctx->num_sms * std::max(1, bpsY));
-  const int gZ = (int)std::min<long long>(tilesZ, (long long)ctx->num_sms * std::max(1, bpsZ));
-  const StreamMaps &mp = *s->maps;
-  auto step = [&](cudaStream_t q) {
-    if (XG == 16) sx_kernel<8, 16><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
-    else if (K == 8) sx_kernel<8, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
-    else if (K == 12) sx_kernel<12, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
-    else sx_kernel<16, 32><<<gX, 256, xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
-    if (colY) col_launch<false>(S.ny, gY, q, mp.cyA, mp.cyM, mp.cyA, h);
-    else yz_launch<false>(S.ny, gY, q, mp.yA, mp.yM, mp.yA, h);
-    if (colZ) col_launch<true>(S.nz, gZ, q, mp.czA, mp.czM, mp.czT, h);
-    else yz_launch<true>(S.nz, gZ, q, mp.zA, mp.zM, mp.zT, h);
-  };
+  const long long tilesY = (long long)((S.nx + (k.colY ? 31 : kTW - 1)) / (k.colY ? 32 : kTW)) * S.nz;
+  const long long tilesZ = (long long)((S.nx + (k.colZ ? 31 : kTW - 1)) / (k.colZ ? 32 : kTW)) * S.ny;
+  k.gX = (int)std::min<long long>(tilesX, (long long)ctx->num_sms * xbps);
+  k.gY = (int)std::min<long long>(tilesY, (long long)ctx->num_sms * std::max(1, bpsY));
+  k.gZ = (int)std::min<long long>(tilesZ, (long long)ctx->num_sms * std::max(1, bpsZ));
+  return MCB_OK;
+}
+
+// Enqueues one DG-ADI step (X, Y and Z passes).
+void stream_step_launch(const StreamStepper &k, cudaStream_t q) {
+  const StreamMaps &mp = *k.maps;
+  const StreamDev &h = k.h;
+  const StreamShape &S = k.S;
+  if (k.XG == 16) sx_kernel<8, 16><<<k.gX, 256, k.xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+  else if (k.K == 8) sx_kernel<8, 32><<<k.gX, 256, k.xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+  else if (k.K == 12) sx_kernel<12, 32><<<k.gX, 256, k.xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+  else sx_kernel<16, 32><<<k.gX, 256, k.xs, q>>>(mp.xTh, mp.xTr, mp.xQr, mp.xMh, mp.xCr, h);
+  if (k.colY) col_launch<false>(S.ny, k.gY, q, mp.cyA, mp.cyM, mp.cyA, h);
+  else yz_launch<false>(S.ny, k.gY, q, mp.yA, mp.yM, mp.yA, h);
+  if (k.colZ) col_launch<true>(S.nz, k.gZ, q, mp.czA, mp.czM, mp.czT, h);
+  else yz_launch<true>(S.nz, k.gZ, q, mp.zA, mp.zM, mp.zT, h);
+}
+
+mcb_status stream_stepper_new(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, StreamStepper **out) {
+  StreamStepper *k = new StreamStepper();
+  const mcb_status rc = stream_setup(ctx, s, p, nullptr, k);
+  if (rc != MCB_OK) {
+    delete k;
+    return rc;
+  }
+  *out = k;
+  return MCB_OK;
+}
+
+void stream_stepper_free(StreamStepper *k) { delete k; }
+
+void stream_stepper_launch(const StreamStepper *k, cudaStream_t st) { stream_step_launch(*k, st); }
+
+void stream_dense_copy(mcb_ctx *ctx, const mcb_heat_state *s, float *dense, cudaStream_t st) {
+  const StreamShape &S = s->shape;
+  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, dense, 0.0, Pitch{S.nx, S.ny, S.nz, S.px},
+                                                          (long long)S.nx * S.ny * S.nz);
+}
+
+void stream_dense_set(mcb_ctx *ctx, mcb_heat_state *s, const float *dense, cudaStream_t st) {
+  const StreamShape &S = s->shape;
+  to_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(dense, s->T, 0.0, Pitch{S.nx, S.ny, S.nz, S.px},
+                                                        (long long)S.nx * S.ny * S.nz);
+}
+
+long long stream_pitched_index(const mcb_heat_state *s, long long v) {
+  const StreamShape &S = s->shape;
+  const long long nxy = (long long)S.nx * S.ny;
+  const long long iz = v / nxy, r = v - iz * nxy, iy = r / S.nx, ix = r - iy * S.nx;
+  return ix + (iy + iz * S.ny) * S.px;
+}
+
+// Runs p->steps steps on the device-resident streamed state. Sensor and maximum outputs go to
+// host memory; `sens` is the device buffer of the sensor history ([nS x (steps + 1)] doubles).
+mcb_status stream_step(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *p, double *sens, double *sensorTemps,
+                       float *maxMediaTemps, bool graphs) {
+  cudaStream_t st = ctx->stream;
+  const StreamShape &S = s->shape;
+  const long long L = (long long)S.nx * S.ny * S.nz, nt = p->steps;
+  const int nM = p->nM, nS = p->nSensors;
+  StreamStepper ks;
+  MCB_TRY(stream_setup(ctx, s, p, sens, &ks));
+  const StreamDev &h = ks.h;
+  auto step = [&](cudaStream_t q) { stream_step_launch(ks, q); };
   MCB_CUDA(ctx, cudaEventRecord(ctx->ev0, st));
   const int chunk = 16;
   long long done = 0;
