@@ -33,6 +33,7 @@ struct mcb_heat_state {
   mcb::StreamShape shape;
   mcb::StreamMaps *maps = nullptr;
   uint8_t *code = nullptr;
+  uint8_t *uniX = nullptr, *uniY = nullptr, *uniZ = nullptr;  // homogeneous-chunk tables (streamed)
   float *H = nullptr;
   float4 *Hd = nullptr;
   int codeHs = -1;

@@ -122,6 +122,9 @@ struct StreamDev {
   double *sens;
   int *stepCounter;
   int *err;
+  // per-call tables of the homogeneous lane chunks (medium + 1, or 0): X pass [nz][ny][lanes],
+  // column-layout Y and Z passes [nOther][chunks][px] (stream_setup)
+  const uint8_t *uniX, *uniY, *uniZ;
 };
 
 namespace {
@@ -333,13 +336,10 @@ __device__ __forceinline__ void x_line(const StreamDev &h, unsigned char *b, con
   // s - W - 1 .. e - 1), none heat-sinked, none a line end. Their exact pivots lie within rho^(W+1)
   // of the medium's fixed point b*, so every row takes a = c = h and 1 / b' = 1 / b*.
   const int e = min(s + K, nx);
-  bool uni = act && s >= h.W + 1 && e <= nx - 1;
-  for (int i = s - h.W - 1; uni && i <= e; i++) {
-    const int cd = Cr[i];
-    uni = !(cd & kCodeSink) && (i == e || !(cd & 2));
-  }
+  const int um = act ? h.uniX[((long long)z * h.ny + y) * G + lane] : 0;  // uni_x_kernel
+  const bool uni = um != 0;
   if (uni) {
-    const int m0 = Mc[s];
+    const int m0 = um - 1;
     const float ibs = __ldg(&h.Hs[m0].x), f = __ldg(&h.Hd[m0].x) * ibs;
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -744,9 +744,10 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
     // homogeneous lanes: rows s - W - 1 .. e all of one medium, none heat-sinked, none a line end.
     // Their exact pivots lie within rho^(W+1) of the medium's fixed point b* (the recurrence
     // contracts towards it from any start), so every row takes a = c = h, 1 / b' = 1 / b*.
-    bool uni = nv > 0 && !lineSink && s >= h.W + 1 && e <= n - 1;
-    int m0 = uni ? med(s) : 0;
-    for (int i = s - h.W - 1; uni && i <= e; i++) uni = med(i) == m0;
+    // (uni_col_kernel forms the answer once per call)
+    const int um = nv > 0 ? (ZP ? h.uniZ : h.uniY)[((long long)o * G + w) * h.px + x] : 0;
+    const bool uni = um != 0;
+    const int m0 = um - 1;
     if (uni) {
       const float h0 = hd[m0], ibs = hsv[m0], f = h0 * ibs;
       float tPrev = ZP ? Tt[(s - 1) * 32 + l] : 0.f, tCur = ZP ? Tt[s * 32 + l] : 0.f;
@@ -909,6 +910,54 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1)
     for (int k = threadIdx.x; k < nM; k += blockDim.x)
       if (mloc[k]) atomicMax(&h.maxEnc[k], mloc[k]);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(h.stepCounter, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Homogeneous-chunk tables (once per call: they depend on the media, the boundary type and the
+// pivot warm-up length only)
+// ---------------------------------------------------------------------------------------------
+
+// X pass: lane g of the line (y, z) owns rows [g K, g K + K); its chunk is homogeneous when rows
+// s - W - 1 .. e of the line are one medium (code bit 1 clear on rows s - W - 1 .. e - 1), none
+// heat-sinked, none a line end. Entry: medium + 1, or 0.
+__global__ void uni_x_kernel(const StreamDev h, int K, int G, uint8_t *out) {
+  const long long n = (long long)h.ny * h.nz * G;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(t % G);
+    const long long line = t / G;
+    const int y = (int)(line % h.ny), z = (int)(line / h.ny);
+    const long long row = (long long)y * h.px + (long long)z * h.sxy;
+    const int s = g * K, e = min(s + K, h.nx);
+    bool uni = s < h.nx && s >= h.W + 1 && e <= h.nx - 1;
+    for (int i = s - h.W - 1; uni && i <= e; i++) {
+      const int cd = h.code[row + i];
+      uni = !(cd & kCodeSink) && (i == e || !(cd & 2));
+    }
+    const int m0 = uni ? h.M[row + s] : 255;
+    out[t] = (uint8_t)(m0 < 255 ? m0 + 1 : 0);
+  }
+}
+
+// Column-layout Y (ZP false) and Z passes: chunk w of G (kk = ceil(n / G) rows) of the line at
+// column x, other index o. Homogeneous: rows s - W - 1 .. e one medium, the line not heat-sinked,
+// none a line end. Entry [o][w][x]: medium + 1, or 0.
+__global__ void uni_col_kernel(const StreamDev h, bool ZP, int G, uint8_t *out) {
+  const int n = ZP ? h.nz : h.ny, nOther = ZP ? h.ny : h.nz;
+  const int kk = (n + G - 1) / G;
+  const long long st = ZP ? h.sxy : (long long)h.px;
+  const long long cnt = (long long)nOther * G * h.px;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cnt; t += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(t % h.px);
+    const long long ow = t / h.px;
+    const int w = (int)(ow % G), o = (int)(ow / G);
+    const int s = min(w * kk, n), e = min(s + kk, n);
+    const bool lineSink = h.hs && (x == 0 || x == h.nx - 1 || o == 0 || o == nOther - 1);
+    const long long base = x + (ZP ? (long long)o * h.px : (long long)o * h.sxy);
+    bool uni = x < h.nx && e > s && !lineSink && s >= h.W + 1 && e <= n - 1;
+    const int m0 = uni ? h.M[base + s * st] : 255;
+    for (int i = s - h.W - 1; uni && i <= e; i++) uni = h.M[base + i * st] == m0;
+    out[t] = (uint8_t)(uni && m0 < 255 ? m0 + 1 : 0);
   }
 }
 
@@ -1233,6 +1282,10 @@ void stream_carve(const std::function<void *(size_t)> &take, mcb_heat_state *s, 
   s->dmg = (float2 *)take(8 * (size_t)nM);
   s->maxEnc = (unsigned int *)take(4 * (size_t)nM);
   s->step = (int *)take(16);
+  // homogeneous-chunk tables of the X pass and of the column-layout Y and Z passes
+  s->uniX = (uint8_t *)take((size_t)S.ny * S.nz * x_lanes(S.nx));
+  s->uniY = S.ny <= kColMaxN ? (uint8_t *)take((size_t)S.px * S.nz * col_warps(S.ny)) : nullptr;
+  s->uniZ = S.nz <= kColMaxN ? (uint8_t *)take((size_t)S.px * S.ny * col_warps(S.nz)) : nullptr;
   (void)nS;
 }
 
@@ -1324,10 +1377,17 @@ mcb_status stream_setup(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params *
   h.nS = nS; h.sIdx = s->sIdx; h.sW = s->sW; h.sens = sens; h.stepCounter = s->step; h.err = s->step + 1;
   s->lastW = h.W;
 
+  h.uniX = s->uniX;
+  h.uniY = s->uniY;
+  h.uniZ = s->uniZ;
   k.S = S;
   k.maps = s->maps;
   k.K = x_chunk(S.nx);
   k.XG = x_lanes(S.nx);
+  uni_x_kernel<<<ctx->num_sms * 4, 256, 0, st>>>(h, k.K, k.XG, s->uniX);
+  if (s->uniY) uni_col_kernel<<<ctx->num_sms * 4, 256, 0, st>>>(h, false, col_warps(S.ny), s->uniY);
+  if (s->uniZ) uni_col_kernel<<<ctx->num_sms * 4, 256, 0, st>>>(h, true, col_warps(S.nz), s->uniZ);
+  MCB_CUDA(ctx, cudaGetLastError());
   const int XL = x_tile_lines(S.nx);
   k.xs = x_smem(S.px, h.Q != nullptr, S.nx);
   if (k.XG == 16) MCB_TRY((x_attr<8, 16>(ctx, k.xs)));

@@ -60,3 +60,21 @@ def test_gpu_adjoint_checkpoint_count_invariance():
         np.testing.assert_allclose(r["dJ_dc"], runs[0]["dJ_dc"], rtol=1e-12, atol=1e-12 * np.max(np.abs(runs[0]["dJ_dc"])))
         for name in ("dJ_dQ", "dJ_dT0"):
             np.testing.assert_array_equal(r[name], runs[0][name])
+
+
+def test_gpu_adjoint_matches_oracle_large(oracle_lib):
+    """150x120x100 voxels (the 300x300x200 workload's voxel size, a tenth of its voxels) over 60
+    steps with the default sqrt(N) checkpoints, against the FP64 oracle adjoint: objective and
+    every gradient (the printed errors are the margin under the bounds)."""
+    from mcmatlab_b200 import native
+    from oracle import orc
+    case = configs.heat_adjoint_case(shape=(150, 120, 100), size=(0.5, 0.4, 0.3), nt=60)
+    nx, ny, nz = case["n"]
+    J, dc, dQ, dT = orc.oracle_heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"])
+    g = native.heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"])
+    err = {"J_damage": abs(g["J_damage"] - J[1]) / abs(J[1]), "J_peak": abs(g["J_peak"] - J[2]) / abs(J[2])}
+    for name, ref in (("dJ_dc", dc), ("dJ_dQ", dQ), ("dJ_dT0", dT)):
+        err[name] = float(np.max(np.abs(g[name] - ref)) / np.max(np.abs(ref)))
+    print("adjoint 150x120x100 x 60 vs FP64 oracle:", err)
+    assert err["J_damage"] <= TOL_JD and err["J_peak"] <= TOL_J
+    assert max(err["dJ_dc"], err["dJ_dQ"], err["dJ_dT0"]) <= TOL_GRAD, err
