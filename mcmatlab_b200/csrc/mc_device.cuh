@@ -28,6 +28,7 @@ constexpr float kFltEps = 1.1920928955078125e-07f;
 struct Inst {
   int n[3];
   float d[3];
+  float invd[3];  // 1 / d
   int bt;   // boundaryType
   int ffr;  // farFieldRes
   const uint8_t *M0;    // 0-based medium per voxel
@@ -94,10 +95,8 @@ __device__ __forceinline__ float self_phi(float x) {
 struct Photon {
   float i[3], u[3], D[3];
   float dOverU[3];  // d_k / |u_k| (voxel-crossing length along the ray), recomputed when u changes
-  float uOverD[3];  // u_k / d_k
   int j;
-  float mua, mus, g, RI;
-  int cdf;
+  float mua, mus, RI;
   float stepLeft, weight, time;
   bool inside, alive, sameVoxel;
   int med;   // medium of the current voxel
@@ -223,7 +222,6 @@ __device__ __forceinline__ void direction_changed(Photon &P, const Inst &I) {
   for (int k = 0; k < 3; k++) {
     P.D[k] = P.u[k] != 0.f ? (floorf(P.i[k]) + (P.u[k] > 0) - P.i[k]) * I.d[k] / P.u[k] : __int_as_float(0x7f800000);
     P.dOverU[k] = I.d[k] / fabsf(P.u[k]);
-    P.uOverD[k] = P.u[k] / I.d[k];
   }
 }
 
@@ -232,8 +230,6 @@ __device__ __forceinline__ void medium_props(Photon &P, const Inst &I, int m) {
   const float4 mp = I.med[m];
   P.mua = mp.x;
   P.mus = mp.y;
-  P.g = mp.z;
-  P.cdf = I.cdfidx[m];
 }
 
 __device__ __forceinline__ void voxel_props(Photon &P, const Inst &I) {
@@ -492,7 +488,7 @@ __device__ __forceinline__ float propagate(Photon &P, const Inst &I) {
       P.D[k] = P.dOverU[k];
       P.sameVoxel = false;
     } else {
-      P.i[k] += s * P.uOverD[k];
+      P.i[k] += s * (P.u[k] * I.invd[k]);
       if (floorf(P.i[k]) != io) P.i[k] = P.u[k] > 0 ? io + 1 - kFltEps * (fabsf(io) + 1) : io;
       P.D[k] -= s;
     }
@@ -676,12 +672,12 @@ __device__ __forceinline__ bool check_escape(Photon &P, const Inst &I, bool tall
 __device__ __forceinline__ void scatter(Photon &P, const Inst &I) {
   P.nsteps = 0;
   float ct;
-  if (isnan(P.g)) {
+  const float g = I.med[P.med].z;  // the medium's anisotropy (NaN: custom phase function)
+  if (isnan(g)) {
     const float a = rnd(P, I);
-    const int jt = cdf_search(a, kCdfSize - 1, I.CDFs + P.cdf * kCdfSize);
+    const int jt = cdf_search(a, kCdfSize - 1, I.CDFs + I.cdfidx[P.med] * kCdfSize);
     ct = cosf((jt + rnd(P, I)) * kPi / (kCdfSize - 1));
   } else {
-    const float g = P.g;
     if (fabsf(g) == 1.0f) ct = g;
     else if (fabsf(g) <= 3.4526698e-4f) ct = 2 * rnd(P, I) - 1;  // sqrt(FLT_EPSILON)
     else ct = (1 + g * g - sqrf((1 - g * g) / (1 - g + 2 * g * rnd(P, I)))) / (2 * g);

@@ -160,9 +160,9 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
   bool started = false;
   bool retired = false;
   float wfinal = 0.f;
-  double acc = 0.0;
+  float acc = 0.f;  // deposit run in one voxel (a few sub-steps)
   int accj = -1;
-  unsigned long long steps = 0;
+  unsigned int steps = 0;  // this thread's sub-steps (a 32-bit count: about 1e7 per thread at 1e10 packets)
   unsigned long long pid = 0;
   for (;;) {
     // 1. a finished packet: flush its deposit run, then either queue its end-of-life replay
@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
     bool relaunch = false;
     if (!P.alive && started) {
       if (accj >= 0) {
-        atomic_add_f64(&I->NFR[accj], acc);
+        atomic_add_f64(&I->NFR[accj], (double)acc);
         accj = -1;
-        acc = 0.0;
+        acc = 0.f;
       }
       if (GRAD && boxC > 0.f) {
         for (int m = 0; m < nGM; m++) {
@@ -269,20 +269,20 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
           if (boxC > 0.f) sGA[mj * bd + tid] += s * boxC;
         }
         if (P.inside && I->NFR) {
-          double c = 0.0;
+          float c = 0.f;
           bool dep = false;
           if (replay) {
-            c = (double)wfinal * (double)absorb;
+            c = wfinal * absorb;
             dep = true;
           } else if (!I->eol && criteria_met(P, *I)) {
-            c = (double)absorb;
+            c = absorb;
             dep = true;
           }
           if (dep) {
             if (P.j == accj) {
               acc += c;
             } else {
-              if (accj >= 0) atomic_add_f64(&I->NFR[accj], acc);
+              if (accj >= 0) atomic_add_f64(&I->NFR[accj], (double)acc);
               accj = P.j;
               acc = c;
             }
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256, GRAD ? 3 : 4) transport_kernel(KernelArgs
     }
   }
   // lanes leave the loop at different times, so each adds its own count
-  atomicAdd(a.steps, steps);
+  atomicAdd(a.steps, (unsigned long long)steps);
   if (GRAD) {
     if (nGM > 0 && (I->box[1] > I->box[0]))
       for (int q = 0; q < 1 + 2 * nGM; q++) atomicAdd(&sF[q], (double)sBox[q * bd + tid]);
@@ -813,6 +813,7 @@ mcb_status build_plan(mcb_ctx *ctx, Arena &ar, ModelPlan &pl, uint32_t stream) {
     std::memset(&I, 0, sizeof I);
     I.n[0] = m->nx; I.n[1] = m->ny; I.n[2] = m->nz;
     I.d[0] = (float)m->dx; I.d[1] = (float)m->dy; I.d[2] = (float)m->dz;
+    I.invd[0] = (float)(1.0 / m->dx); I.invd[1] = (float)(1.0 / m->dy); I.invd[2] = (float)(1.0 / m->dz);
     I.bt = m->boundaryType;
     I.ffr = m->farFieldRes;
     I.M0 = pl.M0;
