@@ -294,6 +294,9 @@ def run_ours(args):
             c4 = res["cpu_baseline"].pop("heat_c4")
             if "heat_adjoint" in res:
                 res["heat_adjoint"]["cpu_forward"] = c4
+            c2 = res["cpu_baseline"].pop("mc_batched")
+            if "mc_batched" in res and c2:
+                res["mc_batched"]["cpu_baseline"] = c2
         print(json.dumps(res), flush=True)
     state.close()
     if dist:
@@ -301,13 +304,24 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+_SWEEP = {}
+
+
+def sweep_inputs(n_inst, scale):
+    """MEX-level inputs of the batched sweep's instances (prepared once per process)."""
+    key = (n_inst, scale)
+    if key not in _SWEEP:
+        models = configs.batched_sweep(n_instances=n_inst, seed=7, photons=(1e5 * scale, 1e7 * scale))
+        _SWEEP[key] = [mexargs.prepare_mc(x) for x in models]
+    return _SWEEP[key]
+
+
 def batched_sweep_measure(dev, n_inst, scale):
     """Batched sweep (64 seeded instances, grids 64^3..200x200x150, 450-900 nm, 1e5-1e7 packets
     log-uniform, Gaussian beams, half with 64 time bins and cyclic x/y boundaries): one batched
     launch vs the plain kernel launched once per instance."""
     from mcmatlab_b200 import native
-    models = configs.batched_sweep(n_instances=n_inst, seed=7, photons=(1e5 * scale, 1e7 * scale))
-    ins = [mexargs.prepare_mc(x) for x in models]
+    ins = sweep_inputs(n_inst, scale)
     total = float(sum(x["nPhotonsRequested"] for x in ins))
     native.mc_run(dict(ins[0], nPhotonsRequested=1e4), device=dev)
     # warm-up over every instance, so the batch's device buffers are sized before the timed calls
@@ -441,8 +455,26 @@ def cpu_baseline(args, sample_steps):
     c4 = {"value": nx4 * ny4 * nz4 * args.c4_cpu_steps / dt4, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
           "sample": "%d DG-ADI steps of the 300x300x200 heat-adjoint workload (forward only, no damage), reference MEX C "
                     "code (-Ofast -fopenmp) on %d host threads" % (args.c4_cpu_steps, cores)}
+    # the batched sweep's instances one after another on the reference MC, each with 0.5% of its packets
+    # (at least 1e3): packets/s of the sweep's instance mix on the host cores
+    c2 = None
+    if args.c2:
+        R2 = ref.RefMC()
+        tp = ts = 0.0
+        for x in sweep_inputs(args.c2_instances, args.c2_scale):
+            mc_in = dict(x)
+            mc_in["nPhotonsRequested"] = max(1e3, round(0.005 * mc_in["nPhotonsRequested"]))
+            tree = mexargs.mex_model_tree(mc_in)
+            t0 = time.perf_counter()
+            out = R2.run(tree, seed=None)
+            ts += time.perf_counter() - t0
+            tp += float(np.asarray(out["nPhotons"]).ravel()[0])
+        c2 = {"value": tp / ts, "unit": "photon packets/s", "cores": cores, "kind": "reference",
+              "sample": "the %d instances of the batched sweep one after another, 0.5%% of each one's packets "
+                        "(%.2e in all), reference MEX C code (-Ofast -fopenmp) on %d host threads"
+                        % (args.c2_instances, tp, cores)}
     return {"value": N_GRID ** 3 * sample_steps / dtw, "unit": "voxel-updates/s", "cores": cores, "kind": "reference",
-            "heat_c4": c4,
+            "heat_c4": c4, "mc_batched": c2,
             "sample": "%d DG-ADI steps of the same 100^3 workload (light on, damage), reference MEX C code "
                       "(-Ofast -fopenmp) on %d host threads" % (sample_steps, cores),
             "mc": {"value": tm["mc_packets"] / tm["mc_s"], "unit": "photon packets/s", "cores": cores, "kind": "reference",
