@@ -18,10 +18,10 @@
 // row (forward multiplier of row i = cc_{i-1} / b'_{i-1}, backward multiplier = a_{i+1} / b'_i),
 // so the warp-scan solvers of the forward run unchanged. A1 and A2 are not stored by the
 // forward: they follow from T and T' by explicit stencils, A2 = T' - dt/2 D_z (T' - T) and
-// A1 = A2 - dt/2 D_y (A2 - T).
+// A1 = A2 - dt/2 D_y (A2 - T), which the assembly forms in shared memory from its staged planes.
 //
 // Memory: nCheckpoints states of T from the forward sweep, a ring of K + 1 states recomputed
-// per segment (K = ceil(steps / nCheckpoints)), and nine grid-sized work arrays.
+// per segment (K = ceil(steps / nCheckpoints)), and six grid-sized work arrays.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,7 +38,6 @@ constexpr int kAdjMaxMedia = 32;
 struct AdjDev {
   HeatDev h;             // grid, media, coefficients, pivots, boundary type, dt
   const float *Tn, *Tp;  // T^n, T^{n+1} (deviations from the state's base temperature)
-  float *A1, *A2;        // intermediates of step n (reconstructed)
   float *lam;            // lambda^{n+1}; the objective's terms at T^{n+1} are added in place
   float *r1, *r2, *r3;   // adjoints of the three solves' right-hand sides
   float *lamOut;         // lambda^n
@@ -56,38 +55,6 @@ struct AdjDev {
   const int *pStep;  // step (1..steps) at which each peak-list voxel reached its maximum
   int step;          // n + 1 of the step being reversed
 };
-
-// The grid-wide adjoint kernels walk x-rows: block b takes rows b, b + gridDim.x, ... (row =
-// iy + ny * iz) and its threads the x positions of a row, so no voxel index is divided.
-// out = U - dt/2 D_dir (U - T^n): dir 2 gives A2 from U = T^{n+1}, dir 1 gives A1 from U = A2.
-__global__ void adj_recon_kernel(AdjDev a, int dir) {
-  const HeatDev &h = a.h;
-  const float *U = dir == 2 ? a.Tp : a.A2;
-  float *out = dir == 2 ? a.A2 : a.A1;
-  const long long st = dir == 1 ? h.nx : (long long)h.nx * h.ny;
-  const int n = dir == 1 ? h.ny : h.nz;
-  const int rows = h.ny * h.nz;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x)
-  for (int ix = threadIdx.x; ix < h.nx; ix += blockDim.x) {
-    const int iy = row % h.ny, iz = row / h.ny;
-    const long long v = ix + (long long)row * h.nx;
-    const int pos = dir == 1 ? iy : iz;
-    const float u = U[v];
-    float d = 0.f;
-    const int code = h.nb[v];
-    if (!(code & kNbSink) && (code & (dir == 1 ? 12 : 48)) == 0) {
-      // both line neighbours exist and share the medium: one coefficient
-      const float w = u - a.Tn[v];
-      d = cf(h, h.M[v], h.M[v], dir) * ((U[v - st] - a.Tn[v - st]) + (U[v + st] - a.Tn[v + st]) - 2.f * w);
-    } else if (!sinked(h, ix, iy, iz)) {
-      const float w = u - a.Tn[v];
-      const int mi = h.M[v];
-      if (pos > 0) d += cf(h, mi, h.M[v - st], dir) * ((U[v - st] - a.Tn[v - st]) - w);
-      if (pos < n - 1) d += cf(h, mi, h.M[v + st], dir) * ((U[v + st] - a.Tn[v + st]) - w);
-    }
-    out[v] = u - h.hdt * d;
-  }
-}
 
 // Objective terms at T^{n+1}: damage (weight w, increment dt A exp(-E / R Tmid)) contributes
 // w dOmega/dT to lambda' (and, kept in gbuf, the same to lambda^n); a peak-list voxel whose
@@ -233,15 +200,14 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
 }
 
 
-// Running per-voxel maximum over the peak list after forward step `step`.
 // The assembly marching along z: a block owns a 32 x 8 tile of (x, y) columns, one thread per
-// column, and walks the planes iz = 0 .. nz-1. Arrays read with in-plane neighbours are staged in
-// shared memory per plane with a one-voxel halo (r1, T^n and the media on a ring of three planes,
-// which also serves their z neighbours; A1 with its x halo and r2, A2 with their y halos on two
-// planes), r3 and T^{n+1} (z neighbours only) on a ring of three centre tiles. Each array is read
-// from memory once (plus the tile halos) instead of once per neighbour, and the loads of the
-// plane after next are in flight while a plane is assembled. Same arithmetic as
-// adj_assemble_kernel, voxel by voxel.
+// column, and walks the planes of its z chunk. r1, T^n, T^{n+1} and the media are staged in
+// shared memory per plane with a one-voxel halo, on a ring of three planes that also serves their
+// z neighbours; r3 on a ring of three centre tiles, r2 with its y halo on two planes. Each array
+// is read from memory once (plus the tile halos) instead of once per neighbour, and the loads of
+// the plane after next are in flight while a plane is assembled. The step's intermediates are
+// formed per plane from the staged tiles: A2 = T' - dt/2 D_z (T' - T) on the halo tile, then
+// A1 = A2 - dt/2 D_y (A2 - T) on the x-halo rows.
 constexpr int kZX = 32, kZY = 8, kZHX = kZX + 2, kZHY = kZY + 2;
 constexpr int kZHN = kZHX * kZHY;  // halo tile (340)
 constexpr int kZCN = kZX * kZY;    // centre tile (256)
@@ -249,11 +215,30 @@ constexpr int kZA1 = kZY * kZHX;   // x-halo tile (272)
 constexpr int kZR2 = kZHY * kZX;   // y-halo tile (320)
 constexpr int kZChunk = 25;        // planes per block
 
+// out = U - dt/2 D_d (U - T^n) at one voxel along the line direction d, from its value u, T^n
+// value t and medium m and those of its two line neighbours (l, r; has*: the neighbour exists).
+// Both neighbours present in the voxel's own medium take one coefficient; a heat-sinked voxel
+// keeps U.
+__device__ __forceinline__ float recon_point(const HeatDev &h, int d, bool sink, int m, float u, float t, bool hasl,
+                                             int ml, float ul, float tl, bool hasr, int mr, float ur, float tr) {
+  if (sink) return u;
+  const float w = u - t;
+  float dd;
+  if (hasl && hasr && ml == m && mr == m) {
+    dd = cf(h, m, m, d) * ((ul - tl) + (ur - tr) - 2.f * w);
+  } else {
+    dd = 0.f;
+    if (hasl) dd += cf(h, m, ml, d) * ((ul - tl) - w);
+    if (hasr) dd += cf(h, m, mr, d) * ((ur - tr) - w);
+  }
+  return u - h.hdt * dd;
+}
+
 __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   const HeatDev &h = a.h;
   __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
-  __shared__ float sR1[3][kZHN], sTN[3][kZHN], sR3[3][kZCN], sTP[3][kZCN];
-  __shared__ float sA1[2][kZA1], sR2[2][kZR2], sA2[2][kZR2];
+  __shared__ float sR1[3][kZHN], sTN[3][kZHN], sTP[3][kZHN], sR3[3][kZCN];
+  __shared__ float sR2[2][kZR2], sA2[kZHN], sA1[kZA1];
   __shared__ uint8_t sM[3][kZHN + 4];
   const int nM = h.nM, nM2 = nM * nM;
   for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) sdc[k] = 0.0;
@@ -261,18 +246,18 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   const long long sxy = (long long)nx * ny;
   const int x0 = blockIdx.x * kZX, y0 = blockIdx.y * kZY;
   const int t = threadIdx.x, tx = t % kZX, ty = t / kZX;
-  // this thread's staging slots: halo elements t and t + 256 (< 340), centre element t, x-halo
-  // elements t and t + 256 (< 272), y-halo elements t and t + 256 (< 320)
+  // this thread's staging slots: halo elements t and t + 256 (< 340), centre element t, y-halo
+  // elements t and t + 256 (< 320)
   auto hoff = [&](int e, int &x, int &y) { x = x0 - 1 + e % kZHX; y = y0 - 1 + e / kZHX; };
   auto inside = [&](int x, int y) { return x >= 0 && x < nx && y >= 0 && y < ny; };
   // prefetch registers of one plane
-  float pR1[2], pTN[2], pR3, pTP, pA1[2], pR2[2], pA2[2];
+  float pR1[2], pTN[2], pTP[2], pR3, pR2[2];
   int pM[2];
   auto load_ring = [&](int iz) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int e = t + 256 * q;
-      pR1[q] = pTN[q] = 0.f;
+      pR1[q] = pTN[q] = pTP[q] = 0.f;
       pM[q] = 0;
       if (e < kZHN) {
         int x, y;
@@ -281,17 +266,14 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
           const long long v = x + (long long)y * nx + iz * sxy;
           pR1[q] = a.r1[v];
           pTN[q] = a.Tn[v];
+          pTP[q] = a.Tp[v];
           pM[q] = h.M[v];
         }
       }
     }
-    pR3 = pTP = 0.f;
+    pR3 = 0.f;
     const int x = x0 + tx, y = y0 + ty;
-    if (x < nx && y < ny) {
-      const long long v = x + (long long)y * nx + iz * sxy;
-      pR3 = a.r3[v];
-      pTP = a.Tp[v];
-    }
+    if (x < nx && y < ny) pR3 = a.r3[x + (long long)y * nx + iz * sxy];
   };
   auto store_ring = [&](int slot) {
 #pragma unroll
@@ -300,28 +282,20 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
       if (e < kZHN) {
         sR1[slot][e] = pR1[q];
         sTN[slot][e] = pTN[q];
+        sTP[slot][e] = pTP[q];
         sM[slot][e] = (uint8_t)pM[q];
       }
     }
     sR3[slot][t] = pR3;
-    sTP[slot][t] = pTP;
   };
   auto load_single = [&](int iz) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int e = t + 256 * q;
-      pA1[q] = pR2[q] = pA2[q] = 0.f;
-      if (e < kZA1) {
-        const int x = x0 - 1 + e % kZHX, y = y0 + e / kZHX;
-        if (inside(x, y)) pA1[q] = a.A1[x + (long long)y * nx + iz * sxy];
-      }
+      pR2[q] = 0.f;
       if (e < kZR2) {
         const int x = x0 + e % kZX, y = y0 - 1 + e / kZX;
-        if (inside(x, y)) {
-          const long long v = x + (long long)y * nx + iz * sxy;
-          pR2[q] = a.r2[v];
-          pA2[q] = a.A2[v];
-        }
+        if (inside(x, y)) pR2[q] = a.r2[x + (long long)y * nx + iz * sxy];
       }
     }
   };
@@ -329,17 +303,13 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int e = t + 256 * q;
-      if (e < kZA1) sA1[slot][e] = pA1[q];
-      if (e < kZR2) {
-        sR2[slot][e] = pR2[q];
-        sA2[slot][e] = pA2[q];
-      }
+      if (e < kZR2) sR2[slot][e] = pR2[q];
     }
   };
   // this block's planes [z0, z1) (blockIdx.z: z chunks of kZChunk planes, for more blocks in flight)
   const int z0 = blockIdx.z * kZChunk, z1 = min(nz, z0 + kZChunk);
-  // prologue: planes z0 - 1, z0, z0 + 1 of the rings and plane z0 of the single-plane tiles
-  // staged, plane z0 + 2 of the rings and z0 + 1 of the others in flight
+  // prologue: planes z0 - 1, z0, z0 + 1 of the rings and plane z0 of r2 staged, plane z0 + 2 of
+  // the rings and z0 + 1 of r2 in flight
   if (z0 > 0) {
     load_ring(z0 - 1);
     store_ring((z0 - 1) % 3);
@@ -363,13 +333,44 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   for (int iz = z0; iz < z1; iz++) {
     __syncthreads();
     const int sc = iz % 3, sp = (iz + 1) % 3, sm = (iz + 2) % 3, q1 = iz & 1;
+    // A2 of this plane on the halo tile (z neighbours from the ring)
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      if (e < kZHN) {
+        int x, y;
+        hoff(e, x, y);
+        float v = 0.f;
+        if (inside(x, y))
+          v = recon_point(h, 2, sinked(h, x, y, iz), sM[sc][e], sTP[sc][e], sTN[sc][e], iz > 0, sM[sm][e], sTP[sm][e],
+                          sTN[sm][e], iz < nz - 1, sM[sp][e], sTP[sp][e], sTN[sp][e]);
+        sA2[e] = v;
+      }
+    }
+    __syncthreads();
+    // A1 of this plane on the x-halo rows (y neighbours from the A2 tile)
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int e = t + 256 * q;
+      if (e < kZA1) {
+        const int x = x0 - 1 + e % kZHX, y = y0 + e / kZHX;
+        const int hh = e + kZHX;  // the same voxel in the halo tile
+        float v = 0.f;
+        if (inside(x, y))
+          v = recon_point(h, 1, sinked(h, x, y, iz), sM[sc][hh], sA2[hh], sTN[sc][hh], y > 0, sM[sc][hh - kZHX],
+                          sA2[hh - kZHX], sTN[sc][hh - kZHX], y < ny - 1, sM[sc][hh + kZHX], sA2[hh + kZHX],
+                          sTN[sc][hh + kZHX]);
+        sA1[e] = v;
+      }
+    }
+    __syncthreads();
     if (col) {
       const long long v = ix + (long long)iy * nx + iz * sxy;
       const int mv = sM[sc][hc];
       const bool nsv = !sinked(h, ix, iy, iz);
       const float r1v = sR1[sc][hc], r2v = sR2[q1][(ty + 1) * kZX + tx], r3v = sR3[sc][t];
       const float tv = sTN[sc][hc];
-      const float a1v = sA1[q1][ty * kZHX + tx + 1], a2v = sA2[q1][(ty + 1) * kZX + tx], tpv = sTP[sc][t];
+      const float a1v = sA1[ty * kZHX + tx + 1], a2v = sA2[hc], tpv = sTP[sc][hc];
       if (nsv && mv != curM) {
         if (curM >= 0)
           for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
@@ -388,9 +389,9 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
         const float r3zl = sR3[sm][t], r3zr = sR3[sp][t];
         const float txl = sTN[sc][hc - 1], txr = sTN[sc][hc + 1], tyl = sTN[sc][hc - kZHX], tyr = sTN[sc][hc + kZHX];
         const float tzl = sTN[sm][hc], tzr = sTN[sp][hc];
-        const float a1l = sA1[q1][ty * kZHX + tx], a1r = sA1[q1][ty * kZHX + tx + 2];
-        const float a2l = sA2[q1][ty * kZX + tx], a2r = sA2[q1][(ty + 2) * kZX + tx];
-        const float tpl = sTP[sm][t], tpr = sTP[sp][t];
+        const float a1l = sA1[ty * kZHX + tx], a1r = sA1[ty * kZHX + tx + 2];
+        const float a2l = sA2[hc - kZHX], a2r = sA2[hc + kZHX];
+        const float tpl = sTP[sm][hc], tpr = sTP[sp][hc];
         const float qy = dt * r1v - hdt * r2v, qz = dt * r1v - hdt * r3v;
         lam += cx * hdt * (r1xl + r1xr - 2.f * r1v) +
                cy * ((dt * r1yl - hdt * r2yl) + (dt * r1yr - hdt * r2yr) - 2.f * qy) +
@@ -425,9 +426,9 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
             if (nsv) {
               lam -= cf(h, mv, mu, d) * qv;
               float contrib;
-              if (d == 0) contrib = hdt * r1v * ((tu + sA1[q1][ty * kZHX + tx + 1 + side]) - pv);
-              else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((sA2[q1][(ty + 1 + side) * kZX + tx] - tu) - pv);
-              else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((sTP[rs][t] - tu) - pv);
+              if (d == 0) contrib = hdt * r1v * ((tu + sA1[ty * kZHX + tx + 1 + side]) - pv);
+              else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((sA2[hu] - tu) - pv);
+              else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((sTP[rs][hc] - tu) - pv);
               if (mu == mv) same[d] += contrib;
               else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
             }
@@ -438,8 +439,8 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
       }
     }
     __syncthreads();
-    // stage the prefetched planes (ring: iz + 2 into the slot of iz - 1; single tiles: iz + 1)
-    // and start the loads of the next ones
+    // stage the prefetched planes (ring: iz + 2 into the slot of iz - 1; r2: iz + 1) and start
+    // the loads of the next ones
     if (iz + 2 < nz && iz + 2 <= z1) store_ring(sm);
     if (iz + 1 < z1) store_single((iz + 1) & 1);
     if (iz + 3 < nz && iz + 3 <= z1) load_ring(iz + 3);
@@ -452,6 +453,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
     if (sdc[k] != 0.0) atomicAdd(&a.dc[k], sdc[k]);
 }
 
+// Running per-voxel maximum over the peak list after forward step `step`.
 __global__ void peak_track_kernel(const float *T, int nP, const int *idx, float *val, int *at, int step) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nP; k += gridDim.x * blockDim.x) {
     const float t = T[idx[k]];
@@ -530,10 +532,10 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
     heat_state_release(&s);
     return rc;
   }
-  // work memory: checkpoints, the segment ring, nine grid arrays, the lists and accumulators
+  // work memory: checkpoints, the segment ring, six grid arrays, the lists and accumulators
   const size_t grid4 = 4 * (size_t)L;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t bytes = al(grid4) * (size_t)(nSeg + K + 1 + 9) + al(8 * (size_t)nM * nM * 3) + al(16) +
+  const size_t bytes = al(grid4) * (size_t)(nSeg + K + 1 + 6) + al(8 * (size_t)nM * nM * 3) + al(16) +
                        al(12 * (size_t)std::max(nD, 1)) + al(12 * (size_t)std::max(nP, 1)) + al(8 * (size_t)std::max(nP, 1)) +
                        4096;
   void *block = nullptr;
@@ -551,15 +553,12 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   float *ckpt = (float *)take(grid4 * (size_t)nSeg);
   float *ring = (float *)take(grid4 * (size_t)(K + 1));
   AdjDev a{};
-  a.A1 = (float *)take(grid4);
-  a.A2 = (float *)take(grid4);
   a.r1 = (float *)take(grid4);
   a.r2 = (float *)take(grid4);
   a.r3 = (float *)take(grid4);
   float *lamA = (float *)take(grid4);
   float *lamB = (float *)take(grid4);
   float *dQ = (float *)take(grid4);
-  (void)take(grid4);  // spare
   a.dc = (double *)take(8 * (size_t)nM * nM * 3);
   a.Jd = (double *)take(16);
   int *dIdxD = (int *)take(4 * (size_t)std::max(nD, 1));
@@ -622,9 +621,6 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   else rc = adj_setup_yz<8>(ctx, ny, nz);
   if (rc != MCB_OK) return fail(rc);
   const int gridX = ks.gridX, gridYZ = ks.gridYZ;
-  const int gridE = (int)std::min<long long>((long long)ny * nz, (long long)ctx->num_sms * 16);
-  // one thread per x position of a row (a warp multiple, at most 512): no idle second pass
-  const int rowThreads = std::min(512, (nx + 31) / 32 * 32);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
   const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
 
@@ -696,8 +692,6 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       a.lamOut = lamNext;
       a.step = (int)(n + 1);
       if (nD || nP) adj_seed_kernel<<<gridL, 256, 0, st>>>(a);
-      adj_recon_kernel<<<gridE, rowThreads, 0, st>>>(a, 2);
-      adj_recon_kernel<<<gridE, rowThreads, 0, st>>>(a, 1);
       if (tw == 32) adj_launch_yz<32>(a, true, gridYZ, st);
       else if (tw == 16) adj_launch_yz<16>(a, true, gridYZ, st);
       else adj_launch_yz<8>(a, true, gridYZ, st);
