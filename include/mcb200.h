@@ -263,8 +263,9 @@ MCB_API mcb_status mcb_heat_state_destroy(mcb_heat_state *state);
  *     + sum_v peakWeight_v * max_{n = 1..steps} T_v^n
  * and its gradients with respect to the conduction table dTdtperdeltaT (c), the heat source
  * dTdt_abs (Q; zero when the light is off) and the initial temperature. States are checkpointed
- * every K = ceil(steps / nCheckpoints) steps (nCheckpoints <= 0: ceil(sqrt(steps))) and each
- * segment is recomputed once during the reverse sweep. At most 32 media. */
+ * every K = ceil(steps / nCheckpoints) steps (nCheckpoints <= 0: ceil(sqrt(steps))) and the K - 1
+ * inner states of each segment are recomputed once during the reverse sweep; nCheckpoints =
+ * steps stores every state (4 nx ny nz bytes each) and recomputes nothing. At most 32 media. */
 typedef struct {
   const float *damageWeight; /* [nx*ny*nz] or NULL */
   const float *peakWeight;   /* [nx*ny*nz] or NULL */

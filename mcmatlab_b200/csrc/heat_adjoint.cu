@@ -20,8 +20,10 @@
 // forward: they follow from T and T' by explicit stencils, A2 = T' - dt/2 D_z (T' - T) and
 // A1 = A2 - dt/2 D_y (A2 - T), which the assembly forms in shared memory from its staged planes.
 //
-// Memory: nCheckpoints states of T from the forward sweep, a ring of K + 1 states recomputed
-// per segment (K = ceil(steps / nCheckpoints)), and six grid-sized work arrays.
+// Memory: nCheckpoints states of T from the forward sweep and its final state, a ring of the
+// K - 1 inner states of a segment recomputed during the reverse sweep (K = ceil(steps /
+// nCheckpoints); a segment's end states are checkpoints), and six grid-sized work arrays. With
+// nCheckpoints = steps every state is stored and nothing is recomputed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -535,7 +537,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   // work memory: checkpoints, the segment ring, six grid arrays, the lists and accumulators
   const size_t grid4 = 4 * (size_t)L;
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t bytes = al(grid4) * (size_t)(nSeg + K + 1 + 6) + al(8 * (size_t)nM * nM * 3) + al(16) +
+  const size_t bytes = al(grid4) * (size_t)(nSeg + 1 + std::max<long long>(K - 1, 1) + 6) + al(8 * (size_t)nM * nM * 3) + al(16) +
                        al(12 * (size_t)std::max(nD, 1)) + al(12 * (size_t)std::max(nP, 1)) + al(8 * (size_t)std::max(nP, 1)) +
                        4096;
   void *block = nullptr;
@@ -550,8 +552,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
     cur += al(b);
     return (void *)q;
   };
-  float *ckpt = (float *)take(grid4 * (size_t)nSeg);
-  float *ring = (float *)take(grid4 * (size_t)(K + 1));
+  float *ckpt = (float *)take(grid4 * (size_t)(nSeg + 1));  // slot nSeg: the final state
+  float *ring = (float *)take(grid4 * (size_t)std::max<long long>(K - 1, 1));
   AdjDev a{};
   a.r1 = (float *)take(grid4);
   a.r2 = (float *)take(grid4);
@@ -660,34 +662,42 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       if (nP) peak_track_kernel<<<gridL, 256, 0, st>>>(s.T, nP, pIdxD, pVal, pStepD, (int)(n + 1));
     }
   }
+  if (sk) stream_dense_copy(ctx, &ss, ckpt + (size_t)nSeg * L, st);
+  else ADJ_CUDA(cudaMemcpyAsync(ckpt + (size_t)nSeg * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
   ADJ_CUDA(cudaGetLastError());
   ADJ_CUDA(cudaEventRecord(ctx->ev1, st));
   ADJ_CUDA(cudaEventSynchronize(ctx->ev1));
   float msF = 0.f;
   ADJ_CUDA(cudaEventElapsedTime(&msF, ctx->ev0, ctx->ev1));
 
-  // reverse sweep, one recomputed segment at a time
+  // reverse sweep, one segment at a time: its end states are checkpoints seg and seg + 1, its
+  // inner states are recomputed from the first into the ring (the stepper is deterministic, so
+  // they equal the forward sweep's)
   ADJ_CUDA(cudaEventRecord(ctx->ev0, st));
   float *lam = lamA, *lamNext = lamB;
   for (long long seg = nSeg - 1; seg >= 0; seg--) {
     const long long n0 = seg * K, n1 = std::min(n0 + K, nt);
-    ADJ_CUDA(cudaMemcpyAsync(ring, ckpt + (size_t)seg * L, grid4, cudaMemcpyDeviceToDevice, st));
-    if (sk) {
-      stream_dense_set(ctx, &ss, ring, st);
-      for (long long j = 1; j <= n1 - n0; j++) {
-        stream_stepper_launch(sk, st);
-        stream_dense_copy(ctx, &ss, ring + (size_t)j * L, st);
-      }
-    } else {
-      ADJ_CUDA(cudaMemcpyAsync(s.T, ring, grid4, cudaMemcpyDeviceToDevice, st));
-      for (long long j = 1; j <= n1 - n0; j++) {
-        heat_step_launch(ks, st);
-        ADJ_CUDA(cudaMemcpyAsync(ring + (size_t)j * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+    const float *first = ckpt + (size_t)seg * L, *last = ckpt + (size_t)(seg + 1) * L;
+    if (n1 - n0 > 1) {
+      if (sk) {
+        stream_dense_set(ctx, &ss, first, st);
+        for (long long j = 1; j < n1 - n0; j++) {
+          stream_stepper_launch(sk, st);
+          stream_dense_copy(ctx, &ss, ring + (size_t)(j - 1) * L, st);
+        }
+      } else {
+        ADJ_CUDA(cudaMemcpyAsync(s.T, first, grid4, cudaMemcpyDeviceToDevice, st));
+        for (long long j = 1; j < n1 - n0; j++) {
+          heat_step_launch(ks, st);
+          ADJ_CUDA(cudaMemcpyAsync(ring + (size_t)(j - 1) * L, s.T, grid4, cudaMemcpyDeviceToDevice, st));
+        }
       }
     }
+    // state n0 + j of the segment
+    auto state = [&](long long j) { return j == 0 ? first : (j == n1 - n0 ? last : ring + (size_t)(j - 1) * L); };
     for (long long n = n1 - 1; n >= n0; n--) {
-      a.Tn = ring + (size_t)(n - n0) * L;
-      a.Tp = ring + (size_t)(n - n0 + 1) * L;
+      a.Tn = state(n - n0);
+      a.Tp = state(n - n0 + 1);
       a.lam = lam;
       a.lamOut = lamNext;
       a.step = (int)(n + 1);

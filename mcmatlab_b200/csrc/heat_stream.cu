@@ -965,6 +965,9 @@ __global__ void uni_col_kernel(const StreamDev h, bool ZP, int G, uint8_t *out) 
 // Layout conversions and per-call set-up kernels
 // ---------------------------------------------------------------------------------------------
 
+// Pitched layout of a dense grid (x rows padded to px elements). The dense <-> pitched
+// conversions walk one (y, z) row per warp (dense row r starts at r nx, pitched row r at r px),
+// so no element index is divided.
 struct Pitch {
   int nx, ny, nz, px;
   __device__ __forceinline__ long long p(long long v) const {
@@ -974,24 +977,34 @@ struct Pitch {
   }
 };
 
-__global__ void to_pitched_dev_kernel(const float *dense, float *out, double base, Pitch P, long long L) {
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
-    out[P.p(v)] = (float)((double)dense[v] - base);
+template <typename S, typename D, typename F>
+__device__ __forceinline__ void row_walk(const Pitch &P, bool toPitched, const S *src, D *dst, F f) {
+  const long long rows = (long long)P.ny * P.nz;
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
+    const long long d = r * P.nx, q = r * P.px;
+    for (int x = lane; x < P.nx; x += 32) {
+      if (toPitched) dst[q + x] = f(src[d + x]);
+      else dst[d + x] = f(src[q + x]);
+    }
+  }
 }
 
-__global__ void from_pitched_dev_kernel(const float *pitched, float *dense, double base, Pitch P, long long L) {
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
-    dense[v] = (float)((double)pitched[P.p(v)] + base);
+__global__ void to_pitched_dev_kernel(const float *dense, float *out, double base, Pitch P) {
+  row_walk(P, true, dense, out, [base](float v) { return (float)((double)v - base); });
 }
 
-__global__ void to_pitched_f32_kernel(const float *dense, float *out, Pitch P, long long L) {
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
-    out[P.p(v)] = dense[v];
+__global__ void from_pitched_dev_kernel(const float *pitched, float *dense, double base, Pitch P) {
+  row_walk(P, false, pitched, dense, [base](float v) { return (float)((double)v + base); });
 }
 
-__global__ void to_pitched_u8_kernel(const uint8_t *dense, uint8_t *out, Pitch P, long long L) {
-  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < L; v += (long long)gridDim.x * blockDim.x)
-    out[P.p(v)] = dense[v];
+__global__ void to_pitched_f32_kernel(const float *dense, float *out, Pitch P) {
+  row_walk(P, true, dense, out, [](float v) { return v; });
+}
+
+__global__ void to_pitched_u8_kernel(const uint8_t *dense, uint8_t *out, Pitch P) {
+  row_walk(P, true, dense, out, [](uint8_t v) { return v; });
 }
 
 // Neighbourhood code (once per call): bit 2d (2d+1) set when the lower (upper) neighbour along d
@@ -1306,10 +1319,10 @@ mcb_status stream_upload(mcb_ctx *ctx, mcb_heat_state *s, const mcb_heat_params 
   MCB_CUDA(ctx, cudaMemsetAsync(s->M, 0, S.Lp, st));
   MCB_CUDA(ctx, cudaMemsetAsync(s->code, 0, S.Lp, st));
   MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, p->M, L, cudaMemcpyHostToDevice, st));
-  to_pitched_u8_kernel<<<grid, 256, 0, st>>>((const uint8_t *)s->stage, s->M, P, L);
+  to_pitched_u8_kernel<<<grid, 256, 0, st>>>((const uint8_t *)s->stage, s->M, P);
   code_kernel<<<grid, 256, 0, st>>>(s->M, s->code, P, p->heatBoundaryType != 0, L);
   MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, T, 4 * L, cudaMemcpyHostToDevice, st));
-  to_pitched_dev_kernel<<<grid, 256, 0, st>>>(s->stage, s->T, s->base, P, L);
+  to_pitched_dev_kernel<<<grid, 256, 0, st>>>(s->stage, s->T, s->base, P);
   if (s->Om && Omega) MCB_CUDA(ctx, cudaMemcpyAsync(s->Om, Omega, 4 * L, cudaMemcpyHostToDevice, st));
   MCB_CUDA(ctx, cudaGetLastError());
   s->codeHs = (int)(p->heatBoundaryType != 0);
@@ -1322,7 +1335,7 @@ mcb_status stream_upload_q(mcb_ctx *ctx, mcb_heat_state *s, const float *Q) {
   const StreamShape &S = s->shape;
   const long long L = (long long)S.nx * S.ny * S.nz;
   MCB_CUDA(ctx, cudaMemcpyAsync(s->stage, Q, 4 * L, cudaMemcpyHostToDevice, st));
-  to_pitched_f32_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->stage, s->Q, Pitch{S.nx, S.ny, S.nz, S.px}, L);
+  to_pitched_f32_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->stage, s->Q, Pitch{S.nx, S.ny, S.nz, S.px});
   MCB_CUDA(ctx, cudaGetLastError());
   s->qValid = true;
   return MCB_OK;
@@ -1443,14 +1456,12 @@ void stream_stepper_launch(const StreamStepper *k, cudaStream_t st) { stream_ste
 
 void stream_dense_copy(mcb_ctx *ctx, const mcb_heat_state *s, float *dense, cudaStream_t st) {
   const StreamShape &S = s->shape;
-  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, dense, 0.0, Pitch{S.nx, S.ny, S.nz, S.px},
-                                                          (long long)S.nx * S.ny * S.nz);
+  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, dense, 0.0, Pitch{S.nx, S.ny, S.nz, S.px});
 }
 
 void stream_dense_set(mcb_ctx *ctx, mcb_heat_state *s, const float *dense, cudaStream_t st) {
   const StreamShape &S = s->shape;
-  to_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(dense, s->T, 0.0, Pitch{S.nx, S.ny, S.nz, S.px},
-                                                        (long long)S.nx * S.ny * S.nz);
+  to_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(dense, s->T, 0.0, Pitch{S.nx, S.ny, S.nz, S.px});
 }
 
 long long stream_pitched_index(const mcb_heat_state *s, long long v) {
@@ -1520,7 +1531,7 @@ mcb_status stream_download(mcb_ctx *ctx, mcb_heat_state *s, float *T, float *Ome
   cudaStream_t st = ctx->stream;
   const StreamShape &S = s->shape;
   const long long L = (long long)S.nx * S.ny * S.nz;
-  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, s->stage, s->base, Pitch{S.nx, S.ny, S.nz, S.px}, L);
+  from_pitched_dev_kernel<<<ctx->num_sms * 8, 256, 0, st>>>(s->T, s->stage, s->base, Pitch{S.nx, S.ny, S.nz, S.px});
   MCB_CUDA(ctx, cudaGetLastError());
   if (T) MCB_CUDA(ctx, cudaMemcpyAsync(T, s->stage, 4 * L, cudaMemcpyDeviceToHost, st));
   if (Omega && s->Om) MCB_CUDA(ctx, cudaMemcpyAsync(Omega, s->Om, 4 * L, cudaMemcpyDeviceToHost, st));

@@ -100,6 +100,14 @@ def context(device=0):
         return _ctx[device]
 
 
+def release(device=0):
+    """Destroys the device's context, which frees its work buffers (a later call creates a new one)."""
+    with _lock:
+        p = _ctx.pop(device, None)
+    if p is not None:
+        lib().mcb_ctx_destroy(p)
+
+
 def _check(st, ctx):
     if st != 0:
         raise MCBError(st, lib().mcb_last_error(ctx).decode())

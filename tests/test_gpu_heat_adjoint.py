@@ -52,9 +52,11 @@ def test_gpu_adjoint_checkpoint_count_invariance():
     from mcmatlab_b200 import native
     case = _case(shape=(24, 20, 16), size=(0.24, 0.2, 0.16), nt=30, peak=1500.0)
     nx, ny, nz = case["n"]
-    runs = [native.heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"], k) for k in (1, 5, 30, 0)]
-    # the recomputed segments reproduce the forward states bit for bit; only the order of the
-    # FP64 atomic sums (damage objective, dJ/dc) varies between runs
+    # one segment, segments of 6, of 8 (the last one 6), of 2, and every state stored (30)
+    runs = [native.heat_adjoint(case["T0"], case["hp"], nx, ny, nz, case["wd"], case["wp"], k)
+            for k in (1, 5, 4, 29, 30, 0)]
+    # the recomputed inner states of the segments reproduce the forward states bit for bit; only
+    # the order of the FP64 atomic sums (damage objective, dJ/dc) varies between runs
     for r in runs[1:]:
         assert abs(r["J"] - runs[0]["J"]) <= 1e-12 * abs(runs[0]["J"])
         np.testing.assert_allclose(r["dJ_dc"], runs[0]["dJ_dc"], rtol=1e-12, atol=1e-12 * np.max(np.abs(runs[0]["dJ_dc"])))
