@@ -471,6 +471,147 @@ __global__ void fill_kernel(float *p, float v, long long n) {
     p[k] = v;
 }
 
+// Y^T / Z^T solves in the column layout, for lines up to 320 rows: a block of G warps owns 32
+// consecutive x columns of whole lines (Y^T: one z, Z^T: one y); lane l is column x0 + l in every
+// warp and warp w holds rows [w kk, w kk + kk) of its column in registers (kk = ceil(n / G) <= K).
+// A warp reads 128 contiguous bytes per row and array, all its rows' loads in flight at once; the
+// chunk maps of the two scans combine across the warps through shared memory (buffers alternate
+// by tile parity, so two barriers per tile suffice), and the solution leaves with coalesced row
+// stores. Multipliers of the transposed system from the factored state's inverse pivots:
+// forward c_{i-1} / b'_{i-1}, backward a_{i+1} / b'_i (same products as adj_solve_yz_kernel).
+constexpr int kAdjColMaxN = 320;
+int adj_col_rows(int n) { return n <= 256 ? 8 : 16; }
+int adj_col_warps(int n) { return (n + adj_col_rows(n) - 1) / adj_col_rows(n); }
+
+template <int K, bool ZP, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 3 : MAXT <= 512 ? 2 : 1) adj_col_kernel(AdjDev a, int G) {
+  const HeatDev &h = a.h;
+  __shared__ float sH[kAdjMaxMedia * kAdjMaxMedia];  // dt/2 c(mi, mj, d) of this direction
+  __shared__ float2 sums[2][2][32 * 32];              // [tile parity][scan][warp * 32 + lane]
+  const int nx = h.nx, nM = h.nM;
+  const long long sxy = (long long)nx * h.ny;
+  const int n = ZP ? h.nz : h.ny, nOther = ZP ? h.ny : h.nz, d = ZP ? 2 : 1;
+  const long long st = ZP ? sxy : nx;
+  const float *__restrict__ in = ZP ? a.lam : a.r3;
+  float *__restrict__ out = ZP ? a.r3 : a.r2;
+  const float *__restrict__ ibd = h.ib + (size_t)d * sxy * h.nz;
+  for (int k = threadIdx.x; k < nM * nM; k += blockDim.x) sH[k] = h.hdt * h.c[k + d * nM * nM];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int kk = (n + G - 1) / G;
+  const int s = min(w * kk, n), e = min(s + kk, n), cnt = e - s;
+  const int xTiles = (nx + 31) >> 5, nTiles = xTiles * nOther;
+  int it = 0;
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++it) {
+    const int x = ((tile % xTiles) << 5) + l, o = tile / xTiles;
+    const long long base = x + (ZP ? (long long)o * nx : (long long)o * sxy);
+    const bool lineSink = h.hs && (x == 0 || x == nx - 1 || o == 0 || o == nOther - 1);
+    const int nv = x < nx ? cnt : 0;  // rows of this lane
+    auto rowSink = [&](int i) { return lineSink || (h.hs && (i == 0 || i == n - 1)); };
+    float r[K], fm[K], bm[K], ib[K];
+    int mk[K];
+    float ibPrev = 0.f;
+    int mPrev = 0, mNext = 0;
+    if (nv > 0 && s > 0) {
+      ibPrev = ibd[base + (s - 1) * st];
+      mPrev = h.M[base + (s - 1) * st];
+    }
+    if (nv > 0 && e < n) mNext = h.M[base + e * st];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      r[k] = ib[k] = 0.f;
+      mk[k] = 0;
+      if (k < nv) {
+        const long long v = base + (s + k) * st;
+        r[k] = in[v];
+        ib[k] = ibd[v];
+        mk[k] = h.M[v];
+      }
+    }
+    // multipliers (slots past the lane's rows: identity maps, fm = bm = 1 with r = ib = 0) and the
+    // forward chunk map
+    float A = 0.f, B = 1.f;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      fm[k] = bm[k] = 1.f;
+      if (k < nv) {
+        const int i = s + k, mi = mk[k];
+        const int mp = k == 0 ? mPrev : mk[k > 0 ? k - 1 : 0];
+        const float ibp = k == 0 ? ibPrev : ib[k > 0 ? k - 1 : 0];
+        const int mn = k + 1 < nv ? mk[k + 1 < K ? k + 1 : K - 1] : mNext;
+        fm[k] = (i > 0 && !rowSink(i - 1)) ? sH[mp + nM * mi] * ibp : 0.f;
+        bm[k] = (i < n - 1 && !rowSink(i + 1)) ? sH[mn + nM * mi] * ib[k] : 0.f;
+      }
+      A = fmaf(fm[k], A, r[k]);
+      B *= fm[k];
+    }
+    float2 *sF = sums[it & 1][0], *sB = sums[it & 1][1];
+    sF[w * 32 + l] = make_float2(A, B);
+    __syncthreads();
+    float dcar = 0.f;
+    for (int q = 0; q < w; q++) {
+      const float2 m2 = sF[q * 32 + l];
+      dcar = fmaf(m2.y, dcar, m2.x);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      dcar = fmaf(fm[k], dcar, r[k]);
+      r[k] = dcar * ib[k];
+    }
+    // back substitution: chunk map y_in = A + B y_out, combined from the last warp down
+    A = 0.f;
+    B = 1.f;
+#pragma unroll
+    for (int k = K - 1; k >= 0; k--) {
+      A = fmaf(bm[k], A, r[k]);
+      B *= bm[k];
+    }
+    sB[w * 32 + l] = make_float2(A, B);
+    __syncthreads();
+    float tcar = 0.f;
+    for (int q = G - 1; q > w; q--) {
+      const float2 m2 = sB[q * 32 + l];
+      tcar = fmaf(m2.y, tcar, m2.x);
+    }
+#pragma unroll
+    for (int k = K - 1; k >= 0; k--) {
+      tcar = fmaf(bm[k], tcar, r[k]);
+      r[k] = tcar;
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (k < nv) out[base + (s + k) * st] = r[k];
+  }
+}
+
+// Column-layout configurations: 8 rows per lane for lines up to 256 rows (block-size classes
+// 256, 512, 1024 threads), 16 beyond (640).
+template <bool ZP>
+mcb_status adj_col_setup(mcb_ctx *ctx, int n, int *grid) {
+  const int G = adj_col_warps(n);
+  int bps = 0;
+  if (adj_col_rows(n) == 16)
+    MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_col_kernel<16, ZP, 640>, 32 * G, 0));
+  else if (G <= 8)
+    MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_col_kernel<8, ZP, 256>, 32 * G, 0));
+  else if (G <= 16)
+    MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_col_kernel<8, ZP, 512>, 32 * G, 0));
+  else
+    MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_col_kernel<8, ZP, 1024>, 32 * G, 0));
+  if (bps < 1) return set_error(ctx, MCB_ECUDA, "adjoint column solve: no block fits on an SM");
+  *grid = ctx->num_sms * bps;
+  return MCB_OK;
+}
+
+template <bool ZP>
+void adj_col_launch(const AdjDev &a, int n, int grid, cudaStream_t st) {
+  const int G = adj_col_warps(n);
+  if (adj_col_rows(n) == 16) adj_col_kernel<16, ZP, 640><<<grid, 32 * G, 0, st>>>(a, G);
+  else if (G <= 8) adj_col_kernel<8, ZP, 256><<<grid, 32 * G, 0, st>>>(a, G);
+  else if (G <= 16) adj_col_kernel<8, ZP, 512><<<grid, 32 * G, 0, st>>>(a, G);
+  else adj_col_kernel<8, ZP, 1024><<<grid, 32 * G, 0, st>>>(a, G);
+}
+
 template <int TW>
 mcb_status adj_setup_yz(mcb_ctx *ctx, int ny, int nz) {
   MCB_CUDA(ctx, cudaFuncSetAttribute(adj_solve_yz_kernel<TW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -623,6 +764,11 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   else rc = adj_setup_yz<8>(ctx, ny, nz);
   if (rc != MCB_OK) return fail(rc);
   const int gridX = ks.gridX, gridYZ = ks.gridYZ;
+  // Y^T and Z^T in the column layout where the lines are short enough (grid 0: the tiled kernel)
+  int gridColY = 0, gridColZ = 0;
+  if (ny <= kAdjColMaxN) rc = adj_col_setup<false>(ctx, ny, &gridColY);
+  if (rc == MCB_OK && nz <= kAdjColMaxN) rc = adj_col_setup<true>(ctx, nz, &gridColZ);
+  if (rc != MCB_OK) return fail(rc);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
   const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
 
@@ -702,10 +848,12 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       a.lamOut = lamNext;
       a.step = (int)(n + 1);
       if (nD || nP) adj_seed_kernel<<<gridL, 256, 0, st>>>(a);
-      if (tw == 32) adj_launch_yz<32>(a, true, gridYZ, st);
+      if (gridColZ) adj_col_launch<true>(a, nz, gridColZ, st);
+      else if (tw == 32) adj_launch_yz<32>(a, true, gridYZ, st);
       else if (tw == 16) adj_launch_yz<16>(a, true, gridYZ, st);
       else adj_launch_yz<8>(a, true, gridYZ, st);
-      if (tw == 32) adj_launch_yz<32>(a, false, gridYZ, st);
+      if (gridColY) adj_col_launch<false>(a, ny, gridColY, st);
+      else if (tw == 32) adj_launch_yz<32>(a, false, gridYZ, st);
       else if (tw == 16) adj_launch_yz<16>(a, false, gridYZ, st);
       else adj_launch_yz<8>(a, false, gridYZ, st);
       adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
