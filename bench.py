@@ -397,7 +397,6 @@ def adjoint_measure(dev, nt):
                              "adjoint_over_forward": (ga["forwardMs"] + ga["adjointMs"]) / fwd_ms,
                              "max_rel_diff_dJ_dT0": float(np.max(np.abs(ga["dJ_dT0"] - g["dJ_dT0"])) /
                                                           np.max(np.abs(g["dJ_dT0"])))}
-        native.release(dev)  # frees the stored states
     return res
 
 

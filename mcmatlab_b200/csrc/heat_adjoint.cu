@@ -471,6 +471,86 @@ __global__ void fill_kernel(float *p, float v, long long n) {
     p[k] = v;
 }
 
+// X^T solve, one warp per x-line (lines up to 512 voxels): the line's right-hand side, inverse
+// pivots and media are read coalesced into the warp's slice of shared memory (element i at
+// i + i / 32, so the lanes' chunk reads fall in distinct banks), lane g solves rows [g K, g K + K)
+// in registers (chunk_solve over the 32 lanes, transposed multipliers as in adj_solve_x_kernel),
+// and the solution leaves through the same slice with coalesced stores.
+constexpr int kAdjXWarps = 4;
+int adj_xline_rows(int nx) { return nx <= 128 ? 4 : nx <= 256 ? 8 : nx <= 384 ? 12 : 16; }
+
+template <int K>
+__global__ void __launch_bounds__(32 * kAdjXWarps, K <= 8 ? 8 : 4) adj_xline_kernel(AdjDev a) {
+  constexpr int NS = 32 * K + K;  // skewed slice length
+  const HeatDev &h = a.h;
+  __shared__ float sH[kAdjMaxMedia * kAdjMaxMedia];  // dt/2 c(mi, mj, x)
+  __shared__ float sR[kAdjXWarps][NS], sI[kAdjXWarps][NS];
+  __shared__ int sM[kAdjXWarps][NS];
+  const int nx = h.nx, ny = h.ny, nz = h.nz, nM = h.nM;
+  for (int k = threadIdx.x; k < nM * nM; k += blockDim.x) sH[k] = h.hdt * h.c[k];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *R = sR[w], *I = sI[w];
+  int *Mw = sM[w];
+  auto sk = [](int i) { return i + (i >> 5); };
+  const int s = lane * K, nv = max(min(s + K, nx) - s, 0);
+  const long long lines = (long long)ny * nz;
+  const long long nw = (long long)gridDim.x * kAdjXWarps;
+  for (long long line = (long long)blockIdx.x * kAdjXWarps + w; line < lines; line += nw) {
+    const int iy = (int)(line % ny), iz = (int)(line / ny);
+    const long long row = line * nx;
+    for (int i = lane; i < nx; i += 32) {
+      R[sk(i)] = a.r2[row + i];
+      I[sk(i)] = h.ib[row + i];
+      Mw[sk(i)] = h.M[row + i];
+    }
+    __syncwarp();
+    const bool lineSinked = h.hs && (iy == 0 || iy == ny - 1 || iz == 0 || iz == nz - 1);
+    auto rowSink = [&](int i) { return lineSinked || (h.hs && (i == 0 || i == nx - 1)); };
+    float r[K], fm[K], bm[K], ib[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      fm[k] = bm[k] = 1.f;
+      ib[k] = r[k] = 0.f;
+      if (k < nv) {
+        const int i = s + k, mi = Mw[sk(i)];
+        ib[k] = I[sk(i)];
+        r[k] = R[sk(i)];
+        fm[k] = (i > 0 && !rowSink(i - 1)) ? sH[Mw[sk(i - 1)] + nM * mi] * I[sk(i - 1)] : 0.f;
+        bm[k] = (i < nx - 1 && !rowSink(i + 1)) ? sH[Mw[sk(i + 1)] + nM * mi] * ib[k] : 0.f;
+      }
+    }
+    chunk_solve<K, 32>(r, fm, bm, ib, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      if (k < nv) R[sk(s + k)] = r[k];
+    __syncwarp();
+    for (int i = lane; i < nx; i += 32) a.r1[row + i] = R[sk(i)];
+    __syncwarp();
+  }
+}
+
+void adj_xline_launch(const AdjDev &a, int grid, cudaStream_t st) {
+  const int K = adj_xline_rows(a.h.nx);
+  if (K == 4) adj_xline_kernel<4><<<grid, 32 * kAdjXWarps, 0, st>>>(a);
+  else if (K == 8) adj_xline_kernel<8><<<grid, 32 * kAdjXWarps, 0, st>>>(a);
+  else if (K == 12) adj_xline_kernel<12><<<grid, 32 * kAdjXWarps, 0, st>>>(a);
+  else adj_xline_kernel<16><<<grid, 32 * kAdjXWarps, 0, st>>>(a);
+}
+
+mcb_status adj_xline_setup(mcb_ctx *ctx, int nx, int *grid) {
+  const int K = adj_xline_rows(nx);
+  int bps = 0;
+  if (K == 4) MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_xline_kernel<4>, 32 * kAdjXWarps, 0));
+  else if (K == 8) MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_xline_kernel<8>, 32 * kAdjXWarps, 0));
+  else if (K == 12) MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_xline_kernel<12>, 32 * kAdjXWarps, 0));
+  else MCB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, adj_xline_kernel<16>, 32 * kAdjXWarps, 0));
+  if (bps < 1) return set_error(ctx, MCB_ECUDA, "adjoint x-line solve: no block fits on an SM");
+  *grid = ctx->num_sms * bps;
+  return MCB_OK;
+}
+
 // Y^T / Z^T solves in the column layout, for lines up to 320 rows: a block of G warps owns 32
 // consecutive x columns of whole lines (Y^T: one z, Z^T: one y); lane l is column x0 + l in every
 // warp and warp w holds rows [w kk, w kk + kk) of its column in registers (kk = ceil(n / G) <= K).
@@ -768,6 +848,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   int gridColY = 0, gridColZ = 0;
   if (ny <= kAdjColMaxN) rc = adj_col_setup<false>(ctx, ny, &gridColY);
   if (rc == MCB_OK && nz <= kAdjColMaxN) rc = adj_col_setup<true>(ctx, nz, &gridColZ);
+  int gridXL = 0;  // X^T one warp per line (grid 0: the tiled kernel)
+  if (rc == MCB_OK && nx <= 512) rc = adj_xline_setup(ctx, nx, &gridXL);
   if (rc != MCB_OK) return fail(rc);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
   const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
@@ -856,7 +938,8 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       else if (tw == 32) adj_launch_yz<32>(a, false, gridYZ, st);
       else if (tw == 16) adj_launch_yz<16>(a, false, gridYZ, st);
       else adj_launch_yz<8>(a, false, gridYZ, st);
-      adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
+      if (gridXL) adj_xline_launch(a, gridXL, st);
+      else adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
       adj_assemble_z_kernel<<<gridZ, 256, 0, st>>>(a);
       if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
       std::swap(lam, lamNext);

@@ -61,6 +61,60 @@ __device__ __forceinline__ bool row_sinked(const HeatDev &h, bool lineSinked, in
   return lineSinked || (h.hs && (i == 0 || i == n - 1));
 }
 
+// Chunked two-scan solve of one line whose lanes hold K consecutive rows each (G lanes per line,
+// an aligned sub-warp group): r (right-hand side in, solution out), fm = a_i / b'_{i-1},
+// bm = c_i / b'_i, ib = 1 / b'_i. Register slots past a lane's rows (a lane may hold fewer than K
+// rows, also in the middle of a line) are identity maps of both scans: fm = bm = 1, ib = r = 0.
+template <int K, int G>
+__device__ __forceinline__ void chunk_solve(float (&r)[K], const float (&fm)[K], const float (&bm)[K], const float (&ib)[K],
+                                            int g) {
+  float A = 0.f, B = 1.f;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    A = fmaf(fm[k], A, r[k]);
+    B *= fm[k];
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Au = __shfl_up_sync(0xffffffffu, A, off, G);
+    const float Bu = __shfl_up_sync(0xffffffffu, B, off, G);
+    if (g >= off) {
+      A = fmaf(B, Au, A);
+      B *= Bu;
+    }
+  }
+  float d = __shfl_up_sync(0xffffffffu, A, 1, G);
+  if (g == 0) d = 0.f;
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    d = fmaf(fm[k], d, r[k]);
+    r[k] = d * ib[k];
+  }
+  A = 0.f;
+  B = 1.f;
+#pragma unroll
+  for (int k = K - 1; k >= 0; k--) {
+    A = fmaf(bm[k], A, r[k]);
+    B *= bm[k];
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    const float Ad = __shfl_down_sync(0xffffffffu, A, off, G);
+    const float Bd = __shfl_down_sync(0xffffffffu, B, off, G);
+    if (g + off < G) {
+      A = fmaf(B, Ad, A);
+      B *= Bd;
+    }
+  }
+  float t = __shfl_down_sync(0xffffffffu, A, 1, G);
+  if (g == G - 1) t = 0.f;
+#pragma unroll
+  for (int k = K - 1; k >= 0; k--) {
+    t = fmaf(bm[k], t, r[k]);
+    r[k] = t;
+  }
+}
+
 // Solves one tridiagonal line with one warp. Shared-memory inputs (element stride st):
 //   rhs  right-hand side, replaced by the solution
 //   fm   forward multipliers  a_i / b'_{i-1}      (Thomas elimination d'_i = rhs_i + fm_i d'_{i-1})

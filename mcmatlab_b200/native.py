@@ -101,7 +101,8 @@ def context(device=0):
 
 
 def release(device=0):
-    """Destroys the device's context, which frees its work buffers (a later call creates a new one)."""
+    """Destroys the device's context, which frees its work buffers (a later call creates a new one).
+    Close every HeatState of the device first: a state keeps a pointer to its context."""
     with _lock:
         p = _ctx.pop(device, None)
     if p is not None:
