@@ -44,6 +44,7 @@ struct AdjDev {
   float *r1, *r2, *r3;   // adjoints of the three solves' right-hand sides
   float *lamOut;         // lambda^n
   float *dQ;             // dJ/dQ accumulator, or nullptr (light off or not requested)
+  int dQinX;             // dQ accumulated by the X^T x-line solve (adj_xline_kernel) instead of the assembly
   double *dc;            // [nM x nM x 3] dJ/dc accumulator
   // objective terms as sparse lists
   int nD;
@@ -221,29 +222,36 @@ constexpr int kZChunk = 25;        // planes per block
 // value t and medium m and those of its two line neighbours (l, r; has*: the neighbour exists).
 // Both neighbours present in the voxel's own medium take one coefficient; a heat-sinked voxel
 // keeps U.
-__device__ __forceinline__ float recon_point(const HeatDev &h, int d, bool sink, int m, float u, float t, bool hasl,
-                                             int ml, float ul, float tl, bool hasr, int mr, float ur, float tr) {
+// C: the conduction table of direction d in shared memory (C[mi + nM mj] = c(mi, mj, d)).
+__device__ __forceinline__ float recon_point(const float *C, int nM, float hdt, bool sink, int m, float u, float t,
+                                             bool hasl, int ml, float ul, float tl, bool hasr, int mr, float ur, float tr) {
   if (sink) return u;
   const float w = u - t;
   float dd;
   if (hasl && hasr && ml == m && mr == m) {
-    dd = cf(h, m, m, d) * ((ul - tl) + (ur - tr) - 2.f * w);
+    dd = C[m + nM * m] * ((ul - tl) + (ur - tr) - 2.f * w);
   } else {
     dd = 0.f;
-    if (hasl) dd += cf(h, m, ml, d) * ((ul - tl) - w);
-    if (hasr) dd += cf(h, m, mr, d) * ((ur - tr) - w);
+    if (hasl) dd += C[m + nM * ml] * ((ul - tl) - w);
+    if (hasr) dd += C[m + nM * mr] * ((ur - tr) - w);
   }
-  return u - h.hdt * dd;
+  return u - hdt * dd;
 }
 
 __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   const HeatDev &h = a.h;
-  __shared__ double sdc[3 * kAdjMaxMedia * kAdjMaxMedia];
+  // dynamic: the dJ/dc block sums [3 nM^2] (double) and the conduction table c [3 nM^2]
+  extern __shared__ double sdc[];
   __shared__ float sR1[3][kZHN], sTN[3][kZHN], sTP[3][kZHN], sR3[3][kZCN];
   __shared__ float sR2[2][kZR2], sA2[kZHN], sA1[kZA1];
   __shared__ uint8_t sM[3][kZHN + 4];
   const int nM = h.nM, nM2 = nM * nM;
-  for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) sdc[k] = 0.0;
+  float *sC = reinterpret_cast<float *>(sdc + 3 * nM2);
+  for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) {
+    sdc[k] = 0.0;
+    sC[k] = h.c[k];
+  }
+  auto cfs = [&](int mi, int mj, int d) { return sC[mi + nM * mj + d * nM2]; };
   const int nx = h.nx, ny = h.ny, nz = h.nz;
   const long long sxy = (long long)nx * ny;
   const int x0 = blockIdx.x * kZX, y0 = blockIdx.y * kZY;
@@ -344,7 +352,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
         hoff(e, x, y);
         float v = 0.f;
         if (inside(x, y))
-          v = recon_point(h, 2, sinked(h, x, y, iz), sM[sc][e], sTP[sc][e], sTN[sc][e], iz > 0, sM[sm][e], sTP[sm][e],
+          v = recon_point(sC + 2 * nM2, nM, hdt, sinked(h, x, y, iz), sM[sc][e], sTP[sc][e], sTN[sc][e], iz > 0, sM[sm][e], sTP[sm][e],
                           sTN[sm][e], iz < nz - 1, sM[sp][e], sTP[sp][e], sTN[sp][e]);
         sA2[e] = v;
       }
@@ -359,7 +367,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
         const int hh = e + kZHX;  // the same voxel in the halo tile
         float v = 0.f;
         if (inside(x, y))
-          v = recon_point(h, 1, sinked(h, x, y, iz), sM[sc][hh], sA2[hh], sTN[sc][hh], y > 0, sM[sc][hh - kZHX],
+          v = recon_point(sC + nM2, nM, hdt, sinked(h, x, y, iz), sM[sc][hh], sA2[hh], sTN[sc][hh], y > 0, sM[sc][hh - kZHX],
                           sA2[hh - kZHX], sTN[sc][hh - kZHX], y < ny - 1, sM[sc][hh + kZHX], sA2[hh + kZHX],
                           sTN[sc][hh + kZHX]);
         sA1[e] = v;
@@ -380,10 +388,14 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
         same[0] = same[1] = same[2] = 0.f;
       }
       float lam = r1v;
-      const bool interior = h.nb[v] == 0 && !(h.hs && (ix <= 1 || ix >= nx - 2 || iy <= 1 || iy >= ny - 2 ||
-                                                       iz <= 1 || iz >= nz - 2));
+      // all six neighbours present, of the voxel's medium, and none of them (nor the voxel)
+      // heat-sinked
+      const int lo = h.hs ? 2 : 1;
+      const bool interior = ix >= lo && ix < nx - lo && iy >= lo && iy < ny - lo && iz >= lo && iz < nz - lo &&
+                            sM[sc][hc - 1] == mv && sM[sc][hc + 1] == mv && sM[sc][hc - kZHX] == mv &&
+                            sM[sc][hc + kZHX] == mv && sM[sm][hc] == mv && sM[sp][hc] == mv;
       if (interior) {
-        const float cx = cf(h, mv, mv, 0), cy = cf(h, mv, mv, 1), cz = cf(h, mv, mv, 2);
+        const float cx = cfs(mv, mv, 0), cy = cfs(mv, mv, 1), cz = cfs(mv, mv, 2);
         const float r1xl = sR1[sc][hc - 1], r1xr = sR1[sc][hc + 1], r1yl = sR1[sc][hc - kZHX],
                     r1yr = sR1[sc][hc + kZHX];
         const float r1zl = sR1[sm][hc], r1zr = sR1[sp][hc];
@@ -402,7 +414,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
         same[1] += dt * r1v * (tyl + tyr - 2.f * tv) + hdt * r2v * ((a2l - tyl) + (a2r - tyr) - 2.f * (a2v - tv));
         same[2] += dt * r1v * (tzl + tzr - 2.f * tv) + hdt * r3v * ((tpl - tzl) + (tpr - tzr) - 2.f * (tpv - tv));
         a.lamOut[v] = lam;
-        if (a.dQ) a.dQ[v] += dt * r1v;
+        if (a.dQ && !a.dQinX) a.dQ[v] += dt * r1v;
       } else {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -423,10 +435,10 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
               const float qu = d == 0   ? hdt * r1u
                                : d == 1 ? dt * r1u - hdt * sR2[q1][(ty + 1 + side) * kZX + tx]
                                         : dt * r1u - hdt * sR3[rs][t];
-              lam += cf(h, mu, mv, d) * qu;
+              lam += cfs(mu, mv, d) * qu;
             }
             if (nsv) {
-              lam -= cf(h, mv, mu, d) * qv;
+              lam -= cfs(mv, mu, d) * qv;
               float contrib;
               if (d == 0) contrib = hdt * r1v * ((tu + sA1[ty * kZHX + tx + 1 + side]) - pv);
               else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((sA2[hu] - tu) - pv);
@@ -437,7 +449,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
           }
         }
         a.lamOut[v] = lam;
-        if (a.dQ && nsv) a.dQ[v] += dt * r1v;
+        if (a.dQ && !a.dQinX && nsv) a.dQ[v] += dt * r1v;
       }
     }
     __syncthreads();
@@ -526,7 +538,11 @@ __global__ void __launch_bounds__(32 * kAdjXWarps, K <= 8 ? 8 : 4) adj_xline_ker
     for (int k = 0; k < K; k++)
       if (k < nv) R[sk(s + k)] = r[k];
     __syncwarp();
-    for (int i = lane; i < nx; i += 32) a.r1[row + i] = R[sk(i)];
+    for (int i = lane; i < nx; i += 32) {
+      const float v = R[sk(i)];
+      a.r1[row + i] = v;
+      if (a.dQ && !rowSink(i)) a.dQ[row + i] += h.dt * v;  // dJ/dQ += dt rho1 (heat-sinked voxels: none)
+    }
     __syncwarp();
   }
 }
@@ -853,6 +869,9 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
   if (rc != MCB_OK) return fail(rc);
   const int gridL = std::max(1, std::min(ctx->num_sms * 4, (std::max(nD, nP) + 255) / 256));
   const dim3 gridZ((nx + kZX - 1) / kZX, (ny + kZY - 1) / kZY, (nz + kZChunk - 1) / kZChunk);
+  const size_t smemZ = (size_t)3 * nM * nM * (8 + 4);
+  ADJ_CUDA(cudaFuncSetAttribute(adj_assemble_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemZ));
+  a.dQinX = gridXL != 0;
 
   // The forward sweeps (checkpoints, segment recomputation) step a streamed state where the grid
   // allows: the same steps up to FP32 rounding at the streamed stepper's speed. The reverse
@@ -940,7 +959,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       else adj_launch_yz<8>(a, false, gridYZ, st);
       if (gridXL) adj_xline_launch(a, gridXL, st);
       else adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
-      adj_assemble_z_kernel<<<gridZ, 256, 0, st>>>(a);
+      adj_assemble_z_kernel<<<gridZ, 256, smemZ, st>>>(a);
       if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
       std::swap(lam, lamNext);
     }
