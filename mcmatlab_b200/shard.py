@@ -9,6 +9,10 @@ wavelength's launched packets, so the merged output is sum_r n_{r,l} out_{r,l} /
 For a fixed packet count the shards together launch exactly the packets of the unsharded run,
 so the merged result equals it up to floating-point summation order.
 
+Perturbation-MC gradient runs shard the same way: their objective values and derivatives are
+means over the launched packets too, so they merge with the same weights, in the same single
+all-reduce as the forward outputs.
+
 Heat is not sharded: its line solves couple whole grid axes (replicas only).
 """
 from __future__ import annotations
@@ -62,6 +66,12 @@ def merge(out, mc_in, rank, world, allreduce):
     submits a buffer of the same length and order whatever its own run produced: an output this
     rank lacks (a rank that ran no packets passes out=None) contributes zeros. Non-finite values
     are reduced as they are, so a NaN on any rank stays NaN in the merge, as combineModels gives."""
+    return _merge(out, mc_in, rank, world, allreduce)[0]
+
+
+def _merge(out, mc_in, rank, world, allreduce, tail=None):
+    """merge() with an optional flat float64 `tail` (already weighted by this rank) appended to
+    the reduced buffer; returns (merged outputs, summed tail or None)."""
     from .abi import result_shapes
     w, nL = _weights(mc_in, rank, world)
     shapes = result_shapes(mc_in)
@@ -78,7 +88,7 @@ def merge(out, mc_in, rank, world, allreduce):
         parts.append((a * w).reshape(-1, order="F"))
     counts = np.array([float(out.get("nPhotons", 0.0)), float(out.get("nPhotonsCollected", 0.0)),
                        float(out.get("nThreads", 0.0))])
-    total = allreduce(np.concatenate(parts + [counts]))
+    total = allreduce(np.concatenate(parts + [counts] + ([] if tail is None else [np.asarray(tail, np.float64)])))
     res = dict(out)
     off = 0
     for k in keys:
@@ -89,7 +99,39 @@ def merge(out, mc_in, rank, world, allreduce):
     res["nPhotons"] = total[off]
     res["nPhotonsCollected"] = total[off + 1]
     res["nThreads"] = total[off + 2]
-    return res
+    return res, (None if tail is None else total[off + 3:])
+
+
+# gradient outputs (mcb_mc_grad_result) in the reduced buffer's order
+GRAD_KEYS = ("R", "dR_dmua", "dR_dmus", "F", "dF_dmua", "dF_dmus")
+
+
+def _grad_shapes(mc_in, nRadialBins):
+    nM = int(np.asarray(mc_in["mua"]).shape[0])
+    return {"R": (nRadialBins,), "dR_dmua": (nRadialBins, nM), "dR_dmus": (nRadialBins, nM), "F": (),
+            "dF_dmua": (nM,), "dF_dmus": (nM,)}
+
+
+def merge_grad(out, g, mc_in, nRadialBins, rank, world, allreduce):
+    """merge() of a gradient run: the forward outputs as merge() does, and the objective values
+    and derivatives (means over the launched packets of the single wavelength) weighted by this
+    rank's share of the packets, all in one all-reduce. A rank without a run passes g=None."""
+    shapes = _grad_shapes(mc_in, nRadialBins)
+    w = _weights(mc_in, rank, world)[0][0]
+    tail = []
+    for k in GRAD_KEYS:
+        n = int(np.prod(shapes[k]))
+        a = None if g is None else g.get(k)
+        tail.append(np.zeros(n) if a is None else w * np.asarray(a, np.float64).reshape(-1, order="F"))
+    res, total = _merge(out, mc_in, rank, world, allreduce, np.concatenate(tail))
+    gm, off = {}, 0
+    for k in GRAD_KEYS:
+        shp = shapes[k]
+        n = int(np.prod(shp))
+        v = total[off:off + n]
+        gm[k] = float(v[0]) if shp == () else v.reshape(shp, order="F").copy()
+        off += n
+    return res, gm
 
 
 def torch_allreduce(group=None):
@@ -129,3 +171,32 @@ def sharded_run(mc_in, rank, world, run, allreduce):
         raise ValueError("nPhotonsRequested must be at least 1")
     out = run(shard_model(mc_in, rank, world)) if shard_count(total, rank, world) > 0 else None
     return merge(out, mc_in, rank, world, allreduce)
+
+
+def sharded_mc_grad(mc_in, nRadialBins=32, radialBinWidth=0.01, box=None, run=None, group=None):
+    """mcb_mc_grad on every rank of `group` (single wavelength): each rank runs its packet shard
+    with `run(mc_in, nRadialBins=, radialBinWidth=, box=)` (default: the CUDA path,
+    native.mc_grad) and all ranks return the merged (outputs, gradients)."""
+    import torch.distributed as dist
+    if run is None:
+        from . import native
+        run = native.mc_grad
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    return sharded_grad_run(mc_in, rank, world, run, torch_allreduce(group), nRadialBins=nRadialBins,
+                            radialBinWidth=radialBinWidth, box=box)
+
+
+def sharded_grad_run(mc_in, rank, world, run, allreduce, nRadialBins=32, radialBinWidth=0.01, box=None):
+    """One rank's part of a sharded gradient run; the checks depend on mc_in only (same answer on
+    every rank, before any work)."""
+    total = float(mc_in["nPhotonsRequested"])
+    if not math.isfinite(total) or mc_in.get("requestCollectedPhotons"):
+        raise ValueError("sharding needs a fixed launched-packet count")
+    if int(total) < 1:
+        raise ValueError("nPhotonsRequested must be at least 1")
+    if np.asarray(mc_in["mua"]).shape[1] != 1:
+        raise ValueError("gradient runs take one wavelength")
+    out, g = None, None
+    if shard_count(total, rank, world) > 0:
+        out, g = run(shard_model(mc_in, rank, world), nRadialBins=nRadialBins, radialBinWidth=radialBinWidth, box=box)
+    return merge_grad(out, g, mc_in, nRadialBins, rank, world, allreduce)

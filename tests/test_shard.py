@@ -139,3 +139,58 @@ def test_merge_layout_is_independent_of_the_rank_outputs():
     shard.merge({"NFR": np.full((2, 2, 2, 1), np.nan), "nPhotons": 1.0, "nPhotonsCollected": 0.0, "nThreads": 1.0},
                 m, 1, 2, fake)
     assert sizes[0] == sizes[1] and sizes[0] > 3
+
+
+def _grad_case():
+    import gradcase
+    mc_in, obj = gradcase.case(n=20, nPhotons=3001)
+    return mc_in, obj
+
+
+def _rank_grad(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import orc
+        mc_in, obj = _grad_case()
+        out, g = shard.sharded_mc_grad(mc_in, run=lambda m, **o: orc.oracle_mc_grad(m, nthreads=2, **o), **obj)
+        if rank == 0:
+            q.put((float(out["nPhotons"]), np.asarray(out["NI_zneg"], np.float64), g))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_merge_gradients_to_the_unsharded_run(oracle_lib):
+    """Perturbation-MC gradients sharded over two gloo ranks (the oracle as each rank's transport):
+    the merged objective values and derivatives equal the unsharded run of the same seed up to
+    floating-point summation order, and so do the forward outputs merged in the same all-reduce."""
+    from oracle import orc
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank_grad, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    nph, ni, g = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    mc_in, obj = _grad_case()
+    full_out, full = orc.oracle_mc_grad(mc_in, nthreads=4, **obj)
+    assert nph == full_out["nPhotons"] == 3001
+    b = np.asarray(full_out["NI_zneg"], np.float64)
+    assert np.max(np.abs(ni - b)) <= 1e-5 * np.max(np.abs(b))
+    assert abs(g["F"] - full["F"]) <= 1e-9 * abs(full["F"])
+    for k in ("R", "dR_dmua", "dR_dmus", "dF_dmua", "dF_dmus"):
+        a, r = np.asarray(g[k], np.float64), np.asarray(full[k], np.float64)
+        assert a.shape == r.shape, k
+        assert np.max(np.abs(a - r)) <= 1e-9 * np.max(np.abs(r)), k
+
+
+def test_gradient_shards_reject_several_wavelengths():
+    mc_in, obj = _grad_case()
+    m = dict(mc_in, mua=np.repeat(np.asarray(mc_in["mua"]), 2, axis=1))
+    with pytest.raises(ValueError):
+        shard.sharded_grad_run(m, 0, 2, None, None, **obj)
