@@ -213,10 +213,11 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
 // A1 = A2 - dt/2 D_y (A2 - T) on the x-halo rows.
 constexpr int kZX = 32, kZY = 8, kZHX = kZX + 2, kZHY = kZY + 2;
 constexpr int kZHN = kZHX * kZHY;  // halo tile (340)
-constexpr int kZCN = kZX * kZY;    // centre tile (256)
+constexpr int kZCN = kZX * kZY;    // centre tile, one thread per column (256)
 constexpr int kZA1 = kZY * kZHX;   // x-halo tile (272)
 constexpr int kZR2 = kZHY * kZX;   // y-halo tile (320)
 constexpr int kZChunk = 25;        // planes per block
+static_assert(kZHN <= 2 * kZCN && kZR2 <= 2 * kZCN && kZA1 <= 2 * kZCN, "two staging slots per thread cover every tile");
 
 // out = U - dt/2 D_d (U - T^n) at one voxel along the line direction d, from its value u, T^n
 // value t and medium m and those of its two line neighbours (l, r; has*: the neighbour exists).
@@ -238,7 +239,7 @@ __device__ __forceinline__ float recon_point(const float *C, int nM, float hdt, 
   return u - hdt * dd;
 }
 
-__global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
+__global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDev a) {
   const HeatDev &h = a.h;
   // dynamic: the dJ/dc block sums [3 nM^2] (double) and the conduction table c [3 nM^2]
   extern __shared__ double sdc[];
@@ -256,8 +257,8 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   const long long sxy = (long long)nx * ny;
   const int x0 = blockIdx.x * kZX, y0 = blockIdx.y * kZY;
   const int t = threadIdx.x, tx = t % kZX, ty = t / kZX;
-  // this thread's staging slots: halo elements t and t + 256 (< 340), centre element t, y-halo
-  // elements t and t + 256 (< 320)
+  // this thread's staging slots: halo elements t and t + kZCN (< kZHN), centre element t, y-halo
+  // elements t and t + kZCN (< kZR2)
   auto hoff = [&](int e, int &x, int &y) { x = x0 - 1 + e % kZHX; y = y0 - 1 + e / kZHX; };
   auto inside = [&](int x, int y) { return x >= 0 && x < nx && y >= 0 && y < ny; };
   // prefetch registers of one plane
@@ -266,7 +267,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   auto load_ring = [&](int iz) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       pR1[q] = pTN[q] = pTP[q] = 0.f;
       pM[q] = 0;
       if (e < kZHN) {
@@ -288,7 +289,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   auto store_ring = [&](int slot) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       if (e < kZHN) {
         sR1[slot][e] = pR1[q];
         sTN[slot][e] = pTN[q];
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   auto load_single = [&](int iz) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       pR2[q] = 0.f;
       if (e < kZR2) {
         const int x = x0 + e % kZX, y = y0 - 1 + e / kZX;
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
   auto store_single = [&](int slot) {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       if (e < kZR2) sR2[slot][e] = pR2[q];
     }
   };
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
     // A2 of this plane on the halo tile (z neighbours from the ring)
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       if (e < kZHN) {
         int x, y;
         hoff(e, x, y);
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(256, 4) adj_assemble_z_kernel(AdjDev a) {
     // A1 of this plane on the x-halo rows (y neighbours from the A2 tile)
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int e = t + 256 * q;
+      const int e = t + kZCN * q;
       if (e < kZA1) {
         const int x = x0 - 1 + e % kZHX, y = y0 + e / kZHX;
         const int hh = e + kZHX;  // the same voxel in the halo tile
@@ -959,7 +960,7 @@ extern "C" mcb_status mcb_heat_adjoint(mcb_ctx *ctx, const mcb_heat_params *pin,
       else adj_launch_yz<8>(a, false, gridYZ, st);
       if (gridXL) adj_xline_launch(a, gridXL, st);
       else adj_solve_x_kernel<<<gridX, 256, smemX, st>>>(a);
-      adj_assemble_z_kernel<<<gridZ, 256, smemZ, st>>>(a);
+      adj_assemble_z_kernel<<<gridZ, kZCN, smemZ, st>>>(a);
       if (nD) adj_damage_tail_kernel<<<gridL, 256, 0, st>>>(a);
       std::swap(lam, lamNext);
     }
