@@ -194,3 +194,26 @@ def test_gradient_shards_reject_several_wavelengths():
     m = dict(mc_in, mua=np.repeat(np.asarray(mc_in["mua"]), 2, axis=1))
     with pytest.raises(ValueError):
         shard.sharded_grad_run(m, 0, 2, None, None, **obj)
+
+
+def test_gradient_merge_of_a_rank_without_packets_contributes_zeros():
+    """A rank with an empty shard submits the same buffer layout as the others (zeros), so the
+    merged gradients are the running rank's values weighted by its full share."""
+    mc_in, obj = _grad_case()
+    mc_in = dict(mc_in, nPhotonsRequested=1.0)
+    nR, nM = obj["nRadialBins"], np.asarray(mc_in["mua"]).shape[0]
+    g0 = {"R": np.arange(nR, dtype=np.float64), "dR_dmua": np.ones((nR, nM)), "dR_dmus": -np.ones((nR, nM)),
+          "F": 2.5, "dF_dmua": np.full(nM, 3.0), "dF_dmus": np.full(nM, -4.0)}
+    bufs = []
+
+    def ar(a):
+        bufs.append(np.array(a))
+        return sum(bufs) if len(bufs) == 2 else a
+    shard.merge_grad({"nPhotons": 1.0}, g0, mc_in, nR, 0, 2, ar)
+    res, g = shard.merge_grad(None, None, mc_in, nR, 1, 2, ar)
+    assert bufs[0].shape == bufs[1].shape
+    assert res["nPhotons"] == 1.0
+    assert g["F"] == 2.5
+    np.testing.assert_array_equal(g["R"], g0["R"])
+    np.testing.assert_array_equal(g["dF_dmus"], g0["dF_dmus"])
+    assert g["dR_dmua"].shape == (nR, nM)
