@@ -48,6 +48,16 @@ def test_gpu_adjoint_matches_oracle_segments(oracle_lib):
     _check(_case(shape=(40, 36, 30), size=(0.4, 0.36, 0.3), nt=50, peak=250.0), nCheckpoints=7)
 
 
+@pytest.mark.parametrize("shape", [(20, 300, 200), (300, 24, 20), (400, 20, 16)])
+def test_gpu_adjoint_line_length_classes(oracle_lib, shape):
+    """The transposed solves' launch classes by line length against the FP64 oracle: y lines of 300
+    rows (16-row lanes) and z lines of 200 (25 warps per line), x lines of 300 and 400 voxels
+    (12 and 16 rows per lane); voxels of 1/300 cm as in the 300x300x200 workload, 8 steps with a
+    heat-sinked boundary."""
+    size = tuple(n / 300.0 for n in shape)
+    _check(_case(shape=shape, size=size, nt=8, hs=1, peak=50.0), nCheckpoints=3)
+
+
 def test_gpu_adjoint_checkpoint_count_invariance():
     from mcmatlab_b200 import native
     case = _case(shape=(24, 20, 16), size=(0.24, 0.2, 0.16), nt=30, peak=1500.0)
