@@ -205,12 +205,12 @@ __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
 
 // The assembly marching along z: a block owns a 32 x 8 tile of (x, y) columns, one thread per
 // column, and walks the planes of its z chunk. r1, T^n, T^{n+1} and the media are staged in
-// shared memory per plane with a one-voxel halo, on a ring of three planes that also serves their
-// z neighbours; r3 on a ring of three centre tiles, r2 with its y halo on two planes. Each array
-// is read from memory once (plus the tile halos) instead of once per neighbour, and the loads of
-// the plane after next are in flight while a plane is assembled. The step's intermediates are
-// formed per plane from the staged tiles: A2 = T' - dt/2 D_z (T' - T) on the halo tile, then
-// A1 = A2 - dt/2 D_y (A2 - T) on the x-halo rows.
+// shared memory per plane with a one-voxel halo, on a ring of four planes that also serves their
+// z neighbours; r3 on a ring of four centre tiles, r2 with its y halo on two planes. Each array
+// is read from memory once (plus the tile halos) instead of once per neighbour, and loads run a
+// plane ahead of the staging. The step's intermediates are formed per plane from the staged
+// tiles, one plane ahead of the assembly (two barriers per plane): A2 = T' - dt/2 D_z (T' - T) on
+// the halo tile, then A1 = A2 - dt/2 D_y (A2 - T) on the x-halo rows.
 constexpr int kZX = 32, kZY = 8, kZHX = kZX + 2, kZHY = kZY + 2;
 constexpr int kZHN = kZHX * kZHY;  // halo tile (340)
 constexpr int kZCN = kZX * kZY;    // centre tile, one thread per column (256)
@@ -243,9 +243,9 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
   const HeatDev &h = a.h;
   // dynamic: the dJ/dc block sums [3 nM^2] (double) and the conduction table c [3 nM^2]
   extern __shared__ double sdc[];
-  __shared__ float sR1[3][kZHN], sTN[3][kZHN], sTP[3][kZHN], sR3[3][kZCN];
-  __shared__ float sR2[2][kZR2], sA2[kZHN], sA1[kZA1];
-  __shared__ uint8_t sM[3][kZHN + 4];
+  __shared__ float sR1[4][kZHN], sTN[4][kZHN], sTP[4][kZHN], sR3[4][kZCN];
+  __shared__ float sR2[2][kZR2], sA2[2][kZHN], sA1[2][kZA1];
+  __shared__ uint8_t sM[4][kZHN + 4];
   const int nM = h.nM, nM2 = nM * nM;
   float *sC = reinterpret_cast<float *>(sdc + 3 * nM2);
   for (int k = threadIdx.x; k < 3 * nM2; k += blockDim.x) {
@@ -319,32 +319,11 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
   };
   // this block's planes [z0, z1) (blockIdx.z: z chunks of kZChunk planes, for more blocks in flight)
   const int z0 = blockIdx.z * kZChunk, z1 = min(nz, z0 + kZChunk);
-  // prologue: planes z0 - 1, z0, z0 + 1 of the rings and plane z0 of r2 staged, plane z0 + 2 of
-  // the rings and z0 + 1 of r2 in flight
-  if (z0 > 0) {
-    load_ring(z0 - 1);
-    store_ring((z0 - 1) % 3);
-  }
-  load_ring(z0);
-  store_ring(z0 % 3);
-  if (z0 + 1 < nz) {
-    load_ring(z0 + 1);
-    store_ring((z0 + 1) % 3);
-  }
-  load_single(z0);
-  store_single(z0 & 1);
-  if (z0 + 2 < nz && z0 + 2 <= z1) load_ring(z0 + 2);
-  if (z0 + 1 < z1) load_single(z0 + 1);
   const float dt = h.dt, hdt = h.hdt;
-  int curM = -1;
-  float same[3] = {0.f, 0.f, 0.f};
-  const int ix = x0 + tx, iy = y0 + ty;
-  const bool col = ix < nx && iy < ny;
-  const int hc = (ty + 1) * kZHX + tx + 1;  // centre in the halo tile
-  for (int iz = z0; iz < z1; iz++) {
-    __syncthreads();
-    const int sc = iz % 3, sp = (iz + 1) % 3, sm = (iz + 2) % 3, q1 = iz & 1;
-    // A2 of this plane on the halo tile (z neighbours from the ring)
+  // A2 of plane p on the halo tile, into sA2[p & 1] (z neighbours from the ring)
+  auto form_a2 = [&](int p) {
+    const int sc = p & 3, sp = (p + 1) & 3, sm = (p + 3) & 3;
+    float *dst = sA2[p & 1];
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int e = t + kZCN * q;
@@ -353,13 +332,17 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
         hoff(e, x, y);
         float v = 0.f;
         if (inside(x, y))
-          v = recon_point(sC + 2 * nM2, nM, hdt, sinked(h, x, y, iz), sM[sc][e], sTP[sc][e], sTN[sc][e], iz > 0, sM[sm][e], sTP[sm][e],
-                          sTN[sm][e], iz < nz - 1, sM[sp][e], sTP[sp][e], sTN[sp][e]);
-        sA2[e] = v;
+          v = recon_point(sC + 2 * nM2, nM, hdt, sinked(h, x, y, p), sM[sc][e], sTP[sc][e], sTN[sc][e], p > 0,
+                          sM[sm][e], sTP[sm][e], sTN[sm][e], p < nz - 1, sM[sp][e], sTP[sp][e], sTN[sp][e]);
+        dst[e] = v;
       }
     }
-    __syncthreads();
-    // A1 of this plane on the x-halo rows (y neighbours from the A2 tile)
+  };
+  // A1 of plane p on the x-halo rows, into sA1[p & 1] (y neighbours from the A2 tile)
+  auto form_a1 = [&](int p) {
+    const int sc = p & 3;
+    const float *A2 = sA2[p & 1];
+    float *dst = sA1[p & 1];
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int e = t + kZCN * q;
@@ -368,20 +351,47 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
         const int hh = e + kZHX;  // the same voxel in the halo tile
         float v = 0.f;
         if (inside(x, y))
-          v = recon_point(sC + nM2, nM, hdt, sinked(h, x, y, iz), sM[sc][hh], sA2[hh], sTN[sc][hh], y > 0, sM[sc][hh - kZHX],
-                          sA2[hh - kZHX], sTN[sc][hh - kZHX], y < ny - 1, sM[sc][hh + kZHX], sA2[hh + kZHX],
-                          sTN[sc][hh + kZHX]);
-        sA1[e] = v;
+          v = recon_point(sC + nM2, nM, hdt, sinked(h, x, y, p), sM[sc][hh], A2[hh], sTN[sc][hh], y > 0,
+                          sM[sc][hh - kZHX], A2[hh - kZHX], sTN[sc][hh - kZHX], y < ny - 1, sM[sc][hh + kZHX],
+                          A2[hh + kZHX], sTN[sc][hh + kZHX]);
+        dst[e] = v;
       }
     }
-    __syncthreads();
+  };
+  // prologue: ring planes z0 - 1 .. z0 + 2 and r2 of plane z0 staged, A2 and A1 of plane z0
+  // formed; ring plane z0 + 3 and r2 of plane z0 + 1 in flight
+  for (int p = max(z0 - 1, 0); p <= min(z0 + 2, min(z1, nz - 1)); p++) {
+    load_ring(p);
+    store_ring(p & 3);
+  }
+  load_single(z0);
+  store_single(z0 & 1);
+  __syncthreads();
+  form_a2(z0);
+  if (z0 + 3 < nz && z0 + 3 <= z1) load_ring(z0 + 3);
+  if (z0 + 1 < z1) load_single(z0 + 1);
+  __syncthreads();
+  form_a1(z0);
+  __syncthreads();
+  int curM = -1;
+  float same[3] = {0.f, 0.f, 0.f};
+  const int ix = x0 + tx, iy = y0 + ty;
+  const bool col = ix < nx && iy < ny;
+  const int hc = (ty + 1) * kZHX + tx + 1;  // centre in the halo tile
+  // per plane, two phases: (1) assemble plane iz and form A2 of plane iz + 1; (2) form A1 of
+  // plane iz + 1, stage the prefetched ring plane iz + 3 (into the slot of iz - 1) and r2 of plane
+  // iz + 1, and start the loads of ring plane iz + 4 and r2 of plane iz + 2
+  for (int iz = z0; iz < z1; iz++) {
+    const int sc = iz & 3, sp = (iz + 1) & 3, sm = (iz + 3) & 3, q1 = iz & 1;
+    const float *A2c = sA2[q1], *A1c = sA1[q1];
+    if (iz + 1 < z1) form_a2(iz + 1);
     if (col) {
       const long long v = ix + (long long)iy * nx + iz * sxy;
       const int mv = sM[sc][hc];
       const bool nsv = !sinked(h, ix, iy, iz);
       const float r1v = sR1[sc][hc], r2v = sR2[q1][(ty + 1) * kZX + tx], r3v = sR3[sc][t];
       const float tv = sTN[sc][hc];
-      const float a1v = sA1[ty * kZHX + tx + 1], a2v = sA2[hc], tpv = sTP[sc][hc];
+      const float a1v = A1c[ty * kZHX + tx + 1], a2v = A2c[hc], tpv = sTP[sc][hc];
       if (nsv && mv != curM) {
         if (curM >= 0)
           for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
@@ -404,8 +414,8 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
         const float r3zl = sR3[sm][t], r3zr = sR3[sp][t];
         const float txl = sTN[sc][hc - 1], txr = sTN[sc][hc + 1], tyl = sTN[sc][hc - kZHX], tyr = sTN[sc][hc + kZHX];
         const float tzl = sTN[sm][hc], tzr = sTN[sp][hc];
-        const float a1l = sA1[ty * kZHX + tx], a1r = sA1[ty * kZHX + tx + 2];
-        const float a2l = sA2[hc - kZHX], a2r = sA2[hc + kZHX];
+        const float a1l = A1c[ty * kZHX + tx], a1r = A1c[ty * kZHX + tx + 2];
+        const float a2l = A2c[hc - kZHX], a2r = A2c[hc + kZHX];
         const float tpl = sTP[sm][hc], tpr = sTP[sp][hc];
         const float qy = dt * r1v - hdt * r2v, qz = dt * r1v - hdt * r3v;
         lam += cx * hdt * (r1xl + r1xr - 2.f * r1v) +
@@ -441,8 +451,8 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
             if (nsv) {
               lam -= cfs(mv, mu, d) * qv;
               float contrib;
-              if (d == 0) contrib = hdt * r1v * ((tu + sA1[ty * kZHX + tx + 1 + side]) - pv);
-              else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((sA2[hu] - tu) - pv);
+              if (d == 0) contrib = hdt * r1v * ((tu + A1c[ty * kZHX + tx + 1 + side]) - pv);
+              else if (d == 1) contrib = dt * r1v * (tu - tv) + hdt * r2v * ((A2c[hu] - tu) - pv);
               else contrib = dt * r1v * (tu - tv) + hdt * r3v * ((sTP[rs][hc] - tu) - pv);
               if (mu == mv) same[d] += contrib;
               else atomicAdd(&sdc[mv + mu * nM + d * nM2], (double)contrib);
@@ -454,12 +464,12 @@ __global__ void __launch_bounds__(kZCN, 1024 / kZCN) adj_assemble_z_kernel(AdjDe
       }
     }
     __syncthreads();
-    // stage the prefetched planes (ring: iz + 2 into the slot of iz - 1; r2: iz + 1) and start
-    // the loads of the next ones
-    if (iz + 2 < nz && iz + 2 <= z1) store_ring(sm);
+    if (iz + 1 < z1) form_a1(iz + 1);
+    if (iz + 3 < nz && iz + 3 <= z1) store_ring((iz + 3) & 3);
     if (iz + 1 < z1) store_single((iz + 1) & 1);
-    if (iz + 3 < nz && iz + 3 <= z1) load_ring(iz + 3);
+    if (iz + 4 < nz && iz + 4 <= z1) load_ring(iz + 4);
     if (iz + 2 < z1) load_single(iz + 2);
+    __syncthreads();
   }
   if (curM >= 0)
     for (int d = 0; d < 3; d++) atomicAdd(&sdc[curM + curM * nM + d * nM2], (double)same[d]);
