@@ -91,7 +91,9 @@ __global__ void adj_damage_tail_kernel(AdjDev a) {
     a.lamOut[a.dIdx[k]] += a.gbuf[k];
 }
 
-// X^T solve: rho1 = X^-T rho2. Same tiling as the forward X pass (h.xl lines per block).
+// X^T solve: rho1 = X^-T rho2, for x lines longer than adj_xline_kernel takes (512 voxels; the
+// assembly then adds dJ/dQ). Same tiling as the factored forward X pass (h.xl lines per block),
+// lines staged in shared memory and solved by solve_lines.
 __global__ void __launch_bounds__(256, 3) adj_solve_x_kernel(AdjDev a) {
   extern __shared__ unsigned char smem[];
   const HeatDev &h = a.h;
@@ -140,8 +142,9 @@ __host__ __device__ constexpr size_t adj_yz_tile_bytes(int n) {
   return (size_t)n * (4 * (TW + 1) * 4 + TW);
 }
 
-// Y^T / Z^T solves: rho2 = Y^-T rho3 (ZPASS false), rho3 = Z^-T lambda' (ZPASS true). Same
-// tiling as the forward Y/Z passes: TW consecutive x positions, one line per x.
+// Y^T / Z^T solves: rho2 = Y^-T rho3 (ZPASS false), rho3 = Z^-T lambda' (ZPASS true), for lines
+// longer than adj_col_kernel takes (320 rows). Same tiling as the factored forward Y/Z passes:
+// TW consecutive x positions, one line per x.
 template <int TW, bool ZPASS>
 __global__ void __launch_bounds__(256, 3) adj_solve_yz_kernel(AdjDev a) {
   extern __shared__ unsigned char smem[];
